@@ -1,0 +1,424 @@
+#!/usr/bin/env python
+"""Range-search throughput benchmark.
+
+Workload (default): 16,000,000 3-D float32 points from 64 Gaussians
+(sigma 0.02, seed 1234) indexed on the device at fan-out 128; each step is
+one batch of 10,000 data-centred cube queries with volumes log-uniform over
+[1e-6, 1e-2] (seed 4321), answered with every query's sorted hit ids.
+
+  value   queries/s, index and query boxes resident in HBM, results left in
+          HBM (one step = qcp_query_batch over the batch)
+  e2e     queries/s through the same public call with host buffers: pinned
+          host boxes in, hit lists out to pinned host memory (both copies
+          inside the timed region)
+  plain   queries/s of the one-query-per-block traversal on the same batch
+
+With torchrun (N ranks) every rank holds the whole index and answers its own
+10,000 queries (weak scaling, no collective on the data path); times are the
+max over ranks.  `--impl reference` times the reference's CPU BVH traversal
+(src/tree/bvh.cpp:165-278, compiled from its sources into oracle/_ref) on
+this host's cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+PKG_DIR = ROOT / "query-co-processing-on-heterogeneous-architectures_b200"
+METRIC = "range queries/sec & p99 ms, batched/served vs plain GPU traversal; HBM GB/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def import_pkg():
+    if "qcp_b200" in sys.modules:
+        return sys.modules["qcp_b200"]
+    spec = importlib.util.spec_from_file_location("qcp_b200", PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["qcp_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def algorithmic_bytes(st: dict, dims: int, fanout: int) -> dict:
+    """Bytes each phase must move at minimum for the work it did:
+    count  leaf-MBR reads of every (query, leaf-parent) item + coordinates of
+           partially covered leaves
+    write  the same reads again + 4 B id read and 4 B id write per hit
+    sort   small slices 8 B/hit (one read, one write), MSD slices 20 B/hit
+    """
+    mbr = st["leaf_items"] * fanout * 2 * dims * 4
+    coords = st["leaves_partial"] * fanout * dims * 4
+    hits = st["hits"]
+    return {"count": mbr + coords, "write": mbr + coords + 8 * hits, "sort": 8 * hits}
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    qcp = import_pkg()
+    import qcp_b200.workloads as W
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    # ---- workload (identical on every rank) --------------------------------
+    q_per_rank = args.queries
+    if args.workload == "uniform1m":
+        w = W.config1()
+        boxes_all = W.fixed_cubes(q_per_rank * world, 3, 0.0464)
+    else:
+        w = W.config2(q=q_per_rank * world)
+        boxes_all = w.boxes
+    boxes = np.ascontiguousarray(boxes_all[rank * q_per_rank:(rank + 1) * q_per_rank])
+    Q = boxes.shape[0]
+
+    d_objs = torch.from_numpy(w.objs).to(dev)
+    d_boxes = torch.from_numpy(boxes).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    torch.cuda.synchronize()
+
+    t0 = time.perf_counter()
+    ix = qcp.Index.build(d_objs, dims=w.dims, n=w.n, fanout=args.fanout, stream=sp)
+    build_ms = (time.perf_counter() - t0) * 1e3
+    info = ix.info()
+    del d_objs
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def step_device(algo, timing):
+        r = ix.search(d_boxes, q=Q, algo=algo, result_mem=qcp.MEM_DEVICE, stream=sp, timing=timing)
+        hits = r.total_hits
+        r.release()
+        return hits
+
+    # ---- value: device-resident -------------------------------------------
+    for _ in range(args.warmup):
+        step_device(args.algo, True)
+    barrier()
+    torch.cuda.synchronize()
+    qcp.launch_count(reset=True)
+    phase = {"expand": 0.0, "count": 0.0, "scan": 0.0, "write": 0.0, "sort": 0.0, "total": 0.0}
+    step_ms = []
+    stats = None
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            e_a = torch.cuda.Event(enable_timing=True)
+            e_b = torch.cuda.Event(enable_timing=True)
+            e_a.record(stream)
+            hits = step_device(args.algo, True)
+            e_b.record(stream)
+            stats = qcp.last_stats()
+            for k in phase:
+                phase[k] += stats[f"ms_{k}"]
+            e_b.synchronize()
+            step_ms.append(e_a.elapsed_time(e_b))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = qcp.launch_count()
+    barrier()
+    elapsed_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    clk = clocks.summary()
+    value = world * Q * args.steps / (elapsed_ms / 1e3)
+
+    # ---- roofline of the dominant kernel ------------------------------------
+    hbm, peak_kind = peaks()
+    dominant = max(["count", "write", "sort"], key=lambda k: phase[k])
+    ab = algorithmic_bytes(stats, w.dims, args.fanout)
+    kernel_names = {"count": "k_leafscan<count>", "write": "k_leafscan<write>",
+                    "sort": "segmented sort (k_sort_small + MSD kernels)"}
+    per_launch_ms = phase[dominant] / args.steps
+    achieved = ab[dominant] / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
+
+    # ---- plain one-query-per-block traversal, same batch -------------------
+    plain = None
+    if args.plain_steps > 0 and args.algo != "plain":
+        step_device("plain", False)
+        torch.cuda.synchronize()
+        e_a = torch.cuda.Event(enable_timing=True)
+        e_b = torch.cuda.Event(enable_timing=True)
+        e_a.record(stream)
+        for _ in range(args.plain_steps):
+            step_device("plain", False)
+        e_b.record(stream)
+        e_b.synchronize()
+        plain_ms = max_over_ranks(e_a.elapsed_time(e_b))
+        plain = world * Q * args.plain_steps / (plain_ms / 1e3)
+
+    # ---- e2e: host buffers through the public call -------------------------
+    h_boxes = torch.from_numpy(boxes).pin_memory()
+    h_np = h_boxes.numpy()
+    h2d = boxes.nbytes
+    d2h = 0
+
+    def step_host():
+        r = ix.search(h_np, algo=args.algo, result_mem=qcp.MEM_HOST, stream=sp, copy=False)
+        nb = (Q + 1) * 8 + r.total_hits * 4
+        r.release()
+        return nb
+
+    for _ in range(max(1, args.warmup // 2)):
+        step_host()
+    barrier()
+    torch.cuda.synchronize()
+    e_a = torch.cuda.Event(enable_timing=True)
+    e_b = torch.cuda.Event(enable_timing=True)
+    e_a.record(stream)
+    for _ in range(args.e2e_steps):
+        d2h = step_host()
+    e_b.record(stream)
+    e_b.synchronize()
+    e2e_ms = max_over_ranks(e_a.elapsed_time(e_b))
+    e2e_value = world * Q * args.e2e_steps / (e2e_ms / 1e3)
+
+    # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w.objs, boxes, args.cpu_seconds)
+
+    ix.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    lat = np.array(step_ms)
+    out = {
+        "metric": METRIC,
+        "value": round(value, 1),
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(elapsed_ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded numpy PCG64; no public dataset)",
+        "config": {
+            "workload": f"{w.name}: {w.n} 3-D points, {Q} queries per GPU per step"
+                        if args.workload != "uniform1m" else f"{w.name}",
+            "fanout": args.fanout, "algo": args.algo, "queries_per_step_per_gpu": Q,
+            "n_objects": w.n, "key": f"hilbert {info['key_bits']} bits/dim",
+            "levels": info["levels"], "index_bytes": info["device_bytes"],
+            "l2": "inputs larger than L2 (index %.0f MB, %.0f MB of ids written per step)"
+                  % (info["device_bytes"] / 1e6, stats["hits"] * 4 / 1e6),
+            "parallelism": f"replicated index, queries sharded over {world} GPU(s)",
+        },
+        "batch_latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
+                             "p99": round(float(np.percentile(lat, 99)), 3)},
+        "hits_per_step": int(stats["hits"]),
+        "build_ms": round(build_ms, 2),
+        "phase_ms_per_step": {k: round(v / args.steps, 4) for k, v in phase.items()},
+        "work_per_step": {k: stats[k] for k in ["leaf_items", "leaves_covered", "leaves_partial",
+                                                 "objects_covered", "sort_small_jobs", "sort_msd_jobs"]},
+        "roofline": {"bound": "hbm", "kernel": kernel_names[dominant],
+                     "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "traffic": None,
+                     "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": int(ab[dominant])},
+        "plain": {"value": round(plain, 1) if plain else None, "unit": "queries/s",
+                  "speedup_batched_vs_plain": round(value / plain, 2) if plain else None},
+        "e2e": {"value": round(e2e_value, 1), "unit": "queries/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
+    print(json.dumps(out), flush=True)
+
+
+def _reference_lib():
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle import Reference  # test infrastructure: the timed reference
+    if not Reference.available(3):
+        return None
+    return Reference(3)
+
+
+def cpu_baseline(objs, boxes, seconds):
+    """The reference's CPU BVH traversal on this host's cores over a bounded
+    sample of the batch (as many queries as fit in about `seconds`)."""
+    ref = _reference_lib()
+    if ref is None:
+        return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    threads = os.cpu_count() or 1
+    h = ref.bvh_build(objs)
+    try:
+        n = min(len(boxes), 256)
+        t = ref.bvh_search_seconds(h, boxes[:n], threads)
+        while t < seconds / 4 and n < len(boxes):
+            n = min(len(boxes), int(n * max(2.0, seconds / max(t, 1e-3) / 2)))
+            t = ref.bvh_search_seconds(h, boxes[:n], threads)
+    finally:
+        ref.bvh_free(h)
+    return {"value": round(n / t, 1), "unit": "queries/s", "cores": threads, "kind": "reference",
+            "sample": f"first {n} of the {len(boxes)} queries of one step, {t:.2f} s, "
+                      f"BVH::Search with {threads} threads"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import qcp_b200.workloads as W  # noqa: F401  (package import below)
+    ref = _reference_lib()
+    if args.workload == "uniform1m":
+        w = W.config1()
+    else:
+        w = W.config2(q=args.queries)
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libqcpref_d3.so not built"}))
+        return
+    threads = os.cpu_count() or 1
+    h = ref.bvh_build(w.objs)
+    boxes = w.boxes
+    # size one step to about args.cpu_seconds of CPU work
+    n = min(len(boxes), 256)
+    t = ref.bvh_search_seconds(h, boxes[:n], threads)
+    while t < args.cpu_seconds / 4 and n < len(boxes):
+        n = min(len(boxes), int(n * max(2.0, args.cpu_seconds / max(t, 1e-3) / 2)))
+        t = ref.bvh_search_seconds(h, boxes[:n], threads)
+    sample = boxes[:n]
+    for _ in range(args.warmup):
+        ref.bvh_search_seconds(h, sample, threads)
+    times = [ref.bvh_search_seconds(h, sample, threads) for _ in range(args.steps)]
+    ref.bvh_free(h)
+    total = sum(times)
+    value = n * len(times) / total
+    print(json.dumps({
+        "impl": "reference",
+        "metric": METRIC, "value": round(value, 1), "unit": "queries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / len(times) * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded numpy PCG64; no public dataset)",
+        "config": {"workload": f"{w.name}: {w.n} 3-D points; each step the first {n} queries of the batch",
+                   "fanout": "reference BVH, <=128 per node"},
+        "cpu_baseline": {"value": round(value, 1), "unit": "queries/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"{n} queries per step, BVH::Search with {threads} threads"},
+        "e2e": {"value": round(value, 1), "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--algo", default="batched", choices=["batched", "plain"])
+    ap.add_argument("--workload", default="gauss16m", choices=["gauss16m", "uniform1m"])
+    ap.add_argument("--queries", type=int, default=10_000)
+    ap.add_argument("--fanout", type=int, default=128)
+    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    rank, world, local = dist_setup(args.gpus)
+    import_pkg()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,193 @@
+/*
+ * qcp.h -- C ABI of the B200 spatial-index range-search library.
+ *
+ * The library builds a bulk-loaded R-tree over points or rectangles on one
+ * GPU (Hilbert keys -> device radix sort -> bottom-up packing) and answers
+ * batches of axis-aligned box queries with the exact hit set of every query
+ * as a sorted list of int32 object ids (0-based input positions).
+ *
+ * Each entry point replaces a piece of the reference's tree interface
+ * (paths inside JinwoongKim/Query-Co-processing-on-Heterogeneous-Architectures):
+ *
+ *   qcp_index_build    tree::Tree::Build            src/tree/tree.h:24
+ *                      (MPHR::Build src/tree/mphr.cpp:35-136 and the
+ *                      ChunkManager::Init/CopyNode residency of
+ *                      src/manager/chunk_manager.cpp:16-40)
+ *   qcp_query_batch    tree::Tree::Search           src/tree/tree.h:47-48
+ *                      (MPHR::Search src/tree/mphr.cpp:196-272), returning
+ *                      per-query id lists instead of a logged hit total
+ *   qcp_query_counts   the per-block hit counters of MPHR::Search
+ *                      (src/tree/mphr.cpp:219-252)
+ *   qcp_index_save     tree::Tree::DumpToFile       src/tree/tree.h:28
+ *   qcp_index_load     tree::Tree::DumpFromFile     src/tree/tree.h:26
+ *   qcp_index_free     the destructors src/tree/mphr.cpp:21-28 (the reference
+ *                      never frees device memory)
+ *   qcp_result_release (no counterpart: the reference returns no lists)
+ *   qcp_last_error     stands in for cudaErrCheck -> exit (src/common/macro.h:100-108)
+ *
+ * Conventions: every call returns a qcp_status and never exits the process;
+ * the caller owns the input buffers; the library owns the index and each
+ * result's buffers until qcp_index_free / qcp_result_release.  Queries on
+ * one index may run concurrently from several host threads; building, saving
+ * or freeing an index must not overlap queries on it.
+ */
+#ifndef QCP_H_
+#define QCP_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum qcp_status {
+  QCP_OK = 0,
+  QCP_ERR_BAD_ARG = 1,         /* invalid argument (message in qcp_last_error) */
+  QCP_ERR_OOM = 2,             /* device or pinned host allocation failed */
+  QCP_ERR_OUTPUT_OVERFLOW = 3, /* a result exceeds the configured output cap */
+  QCP_ERR_TIMEOUT = 4,         /* a bounded device wait ran out */
+  QCP_ERR_CUDA = 5,            /* any other CUDA error */
+  QCP_ERR_NO_DEVICE = 6,       /* no usable CUDA device */
+  QCP_ERR_IO = 7               /* index file could not be read or written */
+} qcp_status;
+
+/* Where a buffer lives. */
+typedef enum qcp_mem { QCP_MEM_HOST = 0, QCP_MEM_DEVICE = 1 } qcp_mem;
+
+/* Hilbert key quantisation. */
+typedef enum qcp_key_mode {
+  /* floor(clamp(p,0,1) * 2^bits) with bits = 32 (2-D), 21 (3-D) or
+   * floor(64/D) otherwise; the default. */
+  QCP_KEY_NORM = 0,
+  /* The reference's key: (long long)(1e6f * p) with 20 bits per dimension
+   * for D > 2 and 31 for D == 2 (src/tree/tree.cpp:597,
+   * src/mapper/hilbert_mapper.cpp:21-23).  Defined for D*bits <= 64. */
+  QCP_KEY_REF = 1
+} qcp_key_mode;
+
+typedef struct qcp_build_opts {
+  uint32_t fanout;    /* entries per node, a multiple of 32 in [32, 256]; 0 = 128 */
+  uint32_t key_mode;  /* qcp_key_mode */
+  uint32_t key_bits;  /* bits per dimension; 0 = the mode's default */
+  uint32_t input_mem; /* qcp_mem of objs */
+  void* stream;       /* cudaStream_t for the build; NULL = legacy default stream */
+} qcp_build_opts;
+
+typedef struct qcp_index qcp_index; /* opaque, device resident */
+
+typedef struct qcp_index_info {
+  uint64_t n;               /* objects indexed */
+  uint32_t dims;
+  uint32_t is_rect;
+  uint32_t fanout;
+  uint32_t levels;          /* tree height; level 0 = leaves */
+  uint64_t level_nodes[16]; /* nodes per level, leaves first */
+  uint64_t device_bytes;    /* bytes of the resident index */
+  uint32_t key_mode;
+  uint32_t key_bits;
+} qcp_index_info;
+
+/* Traversal algorithm. */
+typedef enum qcp_algo {
+  /* All queries of the batch in one work-queue pipeline: level-synchronous
+   * expansion of (query, node) items, then one persistent pass per output
+   * phase with dynamically fetched items; the default. */
+  QCP_ALGO_BATCHED = 0,
+  /* One query per CUDA block, restart-scanning + parent-check traversal
+   * (the reference's MPRS, src/tree/mphr.cpp:303-438), emitting ids. */
+  QCP_ALGO_PLAIN = 1
+} qcp_algo;
+
+typedef struct qcp_query_opts {
+  uint32_t algo;       /* qcp_algo */
+  uint32_t boxes_mem;  /* qcp_mem of the query boxes */
+  uint32_t result_mem; /* qcp_mem where offsets/ids (or counts) are delivered */
+  uint32_t unsorted;   /* 1 = skip the per-query id sort (hit SET still exact) */
+  void* stream;        /* cudaStream_t; NULL = legacy default stream */
+  uint32_t flags;      /* QCP_QUERY_* bits */
+  uint32_t reserved_;
+} qcp_query_opts;
+
+/* flags: record CUDA events around every phase of the call; the times are
+ * reported by qcp_query_stats_last. */
+#define QCP_QUERY_TIMING 1u
+
+/* Work and time of the last query call made on the calling host thread. */
+typedef struct qcp_query_stats {
+  uint32_t algo;
+  uint32_t num_queries;
+  uint64_t frontier_items[16]; /* (query, node) items per level, leaves first */
+  uint64_t leaf_items;         /* (query, leaf-parent) items scanned */
+  uint64_t leaves_covered;     /* overlapping leaves whose MBR lies inside the query */
+  uint64_t leaves_partial;     /* overlapping leaves whose objects were tested */
+  uint64_t objects_covered;    /* objects of covered leaves (hits without a test) */
+  uint64_t hits;
+  uint32_t sort_small_jobs;    /* per-query slices sorted directly */
+  uint32_t sort_msd_jobs;      /* slices split by MSD rounds (all rounds) */
+  /* device milliseconds per phase (only with QCP_QUERY_TIMING) */
+  float ms_expand, ms_count, ms_scan, ms_write, ms_sort, ms_total;
+} qcp_query_stats;
+
+qcp_status qcp_query_stats_last(qcp_query_stats* out);
+
+/* Result of one batch in CSR form: the ids of query i are
+ * ids[offsets[i] .. offsets[i+1]), ascending unless opts.unsorted. */
+typedef struct qcp_result {
+  uint32_t num_queries;
+  uint32_t mem;           /* qcp_mem of offsets and ids */
+  uint64_t total_hits;
+  const uint64_t* offsets; /* num_queries + 1 entries */
+  const int32_t* ids;      /* total_hits entries */
+  void* owner_;            /* library-owned arena; release with qcp_result_release */
+} qcp_result;
+
+/* Build the index.  objs: n rows of dims floats (points, is_rect = 0) or of
+ * 2*dims floats [lo0..lo(D-1), hi0..hi(D-1)] (rectangles, is_rect = 1).
+ * Coordinates must be finite; 1 <= dims <= 8; 1 <= n < 2^31. */
+qcp_status qcp_index_build(const float* objs, uint64_t n, uint32_t dims, uint32_t is_rect,
+                           const qcp_build_opts* opts, qcp_index** out);
+
+qcp_status qcp_index_free(qcp_index* index);
+
+qcp_status qcp_index_get_info(const qcp_index* index, qcp_index_info* info);
+
+/* Run q box queries.  boxes: q rows of 2*dims floats [lo.., hi..]; an object
+ * is a hit iff for every dim d: !(q.lo[d] > e.hi[d] || q.hi[d] < e.lo[d])
+ * (src/node/node_soa.cpp:94-113).  opts may be NULL (batched, host memory,
+ * sorted, default stream).  The call returns after the result is complete. */
+qcp_status qcp_query_batch(qcp_index* index, const float* boxes, uint32_t q,
+                           const qcp_query_opts* opts, qcp_result* out);
+
+/* Hit count of each of q queries into counts[q] (host or device memory per
+ * opts->result_mem). */
+qcp_status qcp_query_counts(qcp_index* index, const float* boxes, uint32_t q,
+                            const qcp_query_opts* opts, uint64_t* counts);
+
+qcp_status qcp_result_release(qcp_result* result);
+
+/* Write the index to a versioned binary file / read it back onto the current
+ * device. */
+qcp_status qcp_index_save(const qcp_index* index, const char* path);
+qcp_status qcp_index_load(const char* path, void* stream, qcp_index** out);
+
+/* Copy the sorted Hilbert keys, the permutation (sorted position -> input id)
+ * and the node MBRs of one level back to host buffers (for tests).  keys
+ * and ids take n entries; mbr takes 2*dims*level_nodes[level] floats laid out
+ * node-major [lo.., hi..].  Any pointer may be NULL. */
+qcp_status qcp_index_export(const qcp_index* index, uint64_t* keys, int32_t* ids,
+                            uint32_t level, float* mbr);
+
+/* Message of the last error on the calling host thread ("" if none). */
+const char* qcp_last_error(void);
+
+/* Kernels this library launched on the calling host thread since the last
+ * reset (reset = 1 clears the counter after reading). */
+uint64_t qcp_launch_count(int reset);
+
+/* Library version string. */
+const char* qcp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QCP_H_ */

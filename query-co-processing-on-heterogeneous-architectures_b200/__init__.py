@@ -1,0 +1,324 @@
+"""B200 range-search library: Python binding of the C ABI in include/qcp.h.
+
+The compute path is the CUDA library libqcp_b200.so next to this file
+(built by the Makefile here, or by __graft_entry__.build()).  This module
+only marshals arguments; there is no CPU fallback, and loading fails loudly
+when the library is missing.
+
+Index mirrors the reference's tree interface (src/tree/tree.h:15-155):
+``Index.build`` stands for Tree::Build, ``Index.search`` for Tree::Search
+(returning per-query id lists instead of a logged total), ``save``/``load``
+for DumpToFile/DumpFromFile.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import pathlib
+
+import numpy as np
+
+PKG_DIR = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libqcp_b200.so"
+
+QCP_OK = 0
+STATUS_NAMES = {
+    0: "QCP_OK", 1: "QCP_ERR_BAD_ARG", 2: "QCP_ERR_OOM", 3: "QCP_ERR_OUTPUT_OVERFLOW",
+    4: "QCP_ERR_TIMEOUT", 5: "QCP_ERR_CUDA", 6: "QCP_ERR_NO_DEVICE", 7: "QCP_ERR_IO",
+}
+MEM_HOST, MEM_DEVICE = 0, 1
+KEY_NORM, KEY_REF = 0, 1
+ALGO_BATCHED, ALGO_PLAIN = 0, 1
+
+
+class QcpError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+class BuildOpts(ctypes.Structure):
+    _fields_ = [("fanout", ctypes.c_uint32), ("key_mode", ctypes.c_uint32),
+                ("key_bits", ctypes.c_uint32), ("input_mem", ctypes.c_uint32),
+                ("stream", ctypes.c_void_p)]
+
+
+class IndexInfo(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint64), ("dims", ctypes.c_uint32), ("is_rect", ctypes.c_uint32),
+                ("fanout", ctypes.c_uint32), ("levels", ctypes.c_uint32),
+                ("level_nodes", ctypes.c_uint64 * 16), ("device_bytes", ctypes.c_uint64),
+                ("key_mode", ctypes.c_uint32), ("key_bits", ctypes.c_uint32)]
+
+
+class QueryOpts(ctypes.Structure):
+    _fields_ = [("algo", ctypes.c_uint32), ("boxes_mem", ctypes.c_uint32),
+                ("result_mem", ctypes.c_uint32), ("unsorted", ctypes.c_uint32),
+                ("stream", ctypes.c_void_p), ("flags", ctypes.c_uint32),
+                ("reserved_", ctypes.c_uint32)]
+
+
+QUERY_TIMING = 1
+
+
+class QueryStats(ctypes.Structure):
+    _fields_ = [("algo", ctypes.c_uint32), ("num_queries", ctypes.c_uint32),
+                ("frontier_items", ctypes.c_uint64 * 16), ("leaf_items", ctypes.c_uint64),
+                ("leaves_covered", ctypes.c_uint64), ("leaves_partial", ctypes.c_uint64),
+                ("objects_covered", ctypes.c_uint64), ("hits", ctypes.c_uint64),
+                ("sort_small_jobs", ctypes.c_uint32), ("sort_msd_jobs", ctypes.c_uint32),
+                ("ms_expand", ctypes.c_float), ("ms_count", ctypes.c_float),
+                ("ms_scan", ctypes.c_float), ("ms_write", ctypes.c_float),
+                ("ms_sort", ctypes.c_float), ("ms_total", ctypes.c_float)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("num_queries", ctypes.c_uint32), ("mem", ctypes.c_uint32),
+                ("total_hits", ctypes.c_uint64), ("offsets", ctypes.c_void_p),
+                ("ids", ctypes.c_void_p), ("owner_", ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
+    """Load libqcp_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = pathlib.Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(
+            f"{p} not found: build it with `make -C {PKG_DIR}` or __graft_entry__.build()")
+    lib = ctypes.CDLL(str(p))
+    P, U32, U64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
+    sig = {
+        "qcp_index_build": ([P, U64, U32, U32, ctypes.POINTER(BuildOpts), ctypes.POINTER(P)], ctypes.c_int),
+        "qcp_index_free": ([P], ctypes.c_int),
+        "qcp_index_get_info": ([P, ctypes.POINTER(IndexInfo)], ctypes.c_int),
+        "qcp_query_batch": ([P, P, U32, ctypes.POINTER(QueryOpts), ctypes.POINTER(Result)], ctypes.c_int),
+        "qcp_query_counts": ([P, P, U32, ctypes.POINTER(QueryOpts), P], ctypes.c_int),
+        "qcp_result_release": ([ctypes.POINTER(Result)], ctypes.c_int),
+        "qcp_index_save": ([P, ctypes.c_char_p], ctypes.c_int),
+        "qcp_index_load": ([ctypes.c_char_p, P, ctypes.POINTER(P)], ctypes.c_int),
+        "qcp_index_export": ([P, P, P, U32, P], ctypes.c_int),
+        "qcp_last_error": ([], ctypes.c_char_p),
+        "qcp_launch_count": ([ctypes.c_int], U64),
+        "qcp_version": ([], ctypes.c_char_p),
+        "qcp_query_stats_last": ([ctypes.POINTER(QueryStats)], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(status: int) -> None:
+    if status != QCP_OK:
+        msg = _lib.qcp_last_error().decode(errors="replace") if _lib else ""
+        raise QcpError(status, msg)
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _device_ptr(t) -> int:
+    """Device address of a CUDA tensor (torch) or an int."""
+    if isinstance(t, int):
+        return t
+    return int(t.data_ptr())
+
+
+class SearchResult:
+    """CSR hit lists: ids of query i are ids[offsets[i]:offsets[i+1]]."""
+
+    def __init__(self, offsets, ids, total_hits: int, mem: int, raw: Result | None = None):
+        self.offsets = offsets
+        self.ids = ids
+        self.total_hits = total_hits
+        self.mem = mem
+        self._raw = raw
+
+    def __len__(self) -> int:
+        return len(self.offsets) - 1 if self.mem == MEM_HOST else int(self._raw.num_queries)
+
+    def hits(self, i: int) -> np.ndarray:
+        return self.ids[self.offsets[i]:self.offsets[i + 1]]
+
+    def counts(self) -> np.ndarray:
+        return np.diff(self.offsets)
+
+    def release(self) -> None:
+        if self._raw is not None and self._raw.owner_:
+            load_library().qcp_result_release(ctypes.byref(self._raw))
+        self._raw = None
+
+
+class Index:
+    """A device-resident bulk-loaded R-tree (one GPU)."""
+
+    def __init__(self, handle: ctypes.c_void_p, dims: int, is_rect: bool):
+        self._h = handle
+        self.dims = dims
+        self.is_rect = is_rect
+
+    # -- construction ---------------------------------------------------------
+    @classmethod
+    def build(cls, objs, dims: int | None = None, is_rect: bool = False, fanout: int = 128,
+              key_mode: int = KEY_NORM, key_bits: int = 0, n: int | None = None,
+              stream: int = 0) -> "Index":
+        """Build from a host numpy array (n x D points or n x 2D rects) or a
+        CUDA tensor / device pointer (then pass n and dims)."""
+        lib = load_library()
+        opts = BuildOpts(fanout, key_mode, key_bits, MEM_HOST, ctypes.c_void_p(stream or None))
+        if isinstance(objs, np.ndarray):
+            a = np.ascontiguousarray(objs, dtype=np.float32)
+            n = a.shape[0]
+            width = a.shape[1]
+            d = width // 2 if is_rect else width
+            if dims is not None and dims != d:
+                raise ValueError("dims does not match the array width")
+            ptr = _ptr(a)
+            keep = a
+        else:
+            if n is None or dims is None:
+                raise ValueError("device input needs n and dims")
+            d = dims
+            opts.input_mem = MEM_DEVICE
+            ptr = ctypes.c_void_p(_device_ptr(objs))
+            keep = objs
+        h = ctypes.c_void_p()
+        _check(lib.qcp_index_build(ptr, n, d, 1 if is_rect else 0, ctypes.byref(opts), ctypes.byref(h)))
+        del keep
+        return cls(h, d, is_rect)
+
+    @classmethod
+    def load(cls, path: str) -> "Index":
+        lib = load_library()
+        h = ctypes.c_void_p()
+        _check(lib.qcp_index_load(str(path).encode(), None, ctypes.byref(h)))
+        idx = cls(h, 0, False)
+        info = idx.info()
+        idx.dims, idx.is_rect = info["dims"], bool(info["is_rect"])
+        return idx
+
+    def save(self, path: str) -> None:
+        _check(load_library().qcp_index_save(self._h, str(path).encode()))
+
+    def close(self) -> None:
+        if self._h:
+            load_library().qcp_index_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- inspection -----------------------------------------------------------
+    def info(self) -> dict:
+        inf = IndexInfo()
+        _check(load_library().qcp_index_get_info(self._h, ctypes.byref(inf)))
+        return {"n": inf.n, "dims": inf.dims, "is_rect": inf.is_rect, "fanout": inf.fanout,
+                "levels": inf.levels, "level_nodes": [inf.level_nodes[i] for i in range(inf.levels)],
+                "device_bytes": inf.device_bytes, "key_mode": inf.key_mode, "key_bits": inf.key_bits}
+
+    def export(self, level: int | None = None):
+        """(sorted keys, sorted-position -> input id, MBRs of `level`)."""
+        inf = self.info()
+        n = inf["n"]
+        keys = np.zeros(n, np.uint64)
+        ids = np.zeros(n, np.int32)
+        mbr = None
+        mptr = None
+        lv = 0
+        if level is not None:
+            lv = level
+            mbr = np.zeros((inf["level_nodes"][level], 2 * inf["dims"]), np.float32)
+            mptr = _ptr(mbr)
+        _check(load_library().qcp_index_export(self._h, _ptr(keys), _ptr(ids), lv, mptr))
+        return keys, ids, mbr
+
+    # -- queries --------------------------------------------------------------
+    def _opts(self, algo, boxes_mem, result_mem, sort, stream, timing=False):
+        a = {"batched": ALGO_BATCHED, "plain": ALGO_PLAIN}.get(algo, algo)
+        return QueryOpts(a, boxes_mem, result_mem, 0 if sort else 1, ctypes.c_void_p(stream or None),
+                         QUERY_TIMING if timing else 0, 0)
+
+    def search(self, boxes, algo="batched", sort: bool = True, result_mem: int = MEM_HOST,
+               q: int | None = None, stream: int = 0, timing: bool = False,
+               copy: bool = True) -> SearchResult:
+        """Run a batch of box queries.  Host numpy boxes (q x 2D) or a CUDA
+        tensor/pointer (then pass q).  Host results are copied into numpy
+        arrays (copy=False: numpy views of the library's pinned result arena,
+        valid until release()); device results stay library-owned until
+        release()."""
+        lib = load_library()
+        if isinstance(boxes, np.ndarray):
+            b = np.ascontiguousarray(boxes, dtype=np.float32).reshape(-1, 2 * self.dims)
+            nq, ptr, bmem = b.shape[0], _ptr(b), MEM_HOST
+        else:
+            if q is None:
+                raise ValueError("device boxes need q")
+            b, nq, ptr, bmem = boxes, q, ctypes.c_void_p(_device_ptr(boxes)), MEM_DEVICE
+        opts = self._opts(algo, bmem, result_mem, sort, stream, timing)
+        r = Result()
+        _check(lib.qcp_query_batch(self._h, ptr, nq, ctypes.byref(opts), ctypes.byref(r)))
+        if result_mem == MEM_HOST and not copy:
+            offs = np.ctypeslib.as_array(ctypes.cast(r.offsets, ctypes.POINTER(ctypes.c_uint64)),
+                                         shape=(nq + 1,))
+            ids = (np.ctypeslib.as_array(ctypes.cast(r.ids, ctypes.POINTER(ctypes.c_int32)),
+                                         shape=(int(r.total_hits),)) if r.total_hits
+                   else np.zeros(0, np.int32))
+            return SearchResult(offs, ids, int(r.total_hits), MEM_HOST, raw=r)
+        if result_mem == MEM_HOST:
+            try:
+                offs = np.ctypeslib.as_array(ctypes.cast(r.offsets, ctypes.POINTER(ctypes.c_uint64)),
+                                             shape=(nq + 1,)).copy()
+                if r.total_hits:
+                    ids = np.ctypeslib.as_array(ctypes.cast(r.ids, ctypes.POINTER(ctypes.c_int32)),
+                                                shape=(int(r.total_hits),)).copy()
+                else:
+                    ids = np.zeros(0, np.int32)
+            finally:
+                lib.qcp_result_release(ctypes.byref(r))
+            return SearchResult(offs, ids, int(r.total_hits), MEM_HOST)
+        return SearchResult(r.offsets, r.ids, int(r.total_hits), MEM_DEVICE, raw=r)
+
+    def counts(self, boxes, algo="batched", q: int | None = None, stream: int = 0) -> np.ndarray:
+        lib = load_library()
+        if isinstance(boxes, np.ndarray):
+            b = np.ascontiguousarray(boxes, dtype=np.float32).reshape(-1, 2 * self.dims)
+            nq, ptr, bmem = b.shape[0], _ptr(b), MEM_HOST
+        else:
+            b, nq, ptr, bmem = boxes, q, ctypes.c_void_p(_device_ptr(boxes)), MEM_DEVICE
+        out = np.zeros(nq, np.uint64)
+        opts = self._opts(algo, bmem, MEM_HOST, True, stream)
+        _check(lib.qcp_query_counts(self._h, ptr, nq, ctypes.byref(opts), _ptr(out)))
+        return out
+
+
+def last_stats() -> dict:
+    """Work counters and (with timing=True) phase times of the last query
+    call on this thread."""
+    st = QueryStats()
+    _check(load_library().qcp_query_stats_last(ctypes.byref(st)))
+    d = {k: getattr(st, k) for k, _ in QueryStats._fields_ if k != "frontier_items"}
+    d["frontier_items"] = list(st.frontier_items)
+    return d
+
+
+def launch_count(reset: bool = False) -> int:
+    """Kernels this library launched on the calling thread."""
+    return int(load_library().qcp_launch_count(1 if reset else 0))

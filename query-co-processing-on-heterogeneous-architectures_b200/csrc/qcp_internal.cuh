@@ -1,0 +1,255 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "qcp.h"
+
+namespace qcp {
+
+constexpr int kMaxLevels = 16;
+constexpr int kMaxDims = 8;
+constexpr uint32_t kWarp = 32;
+
+// ---------------------------------------------------------------------------
+// Errors: every failing step records a message for qcp_last_error and returns
+// a status; nothing exits the process.
+// ---------------------------------------------------------------------------
+void set_error(const std::string& msg);
+void clear_error();
+qcp_status cuda_status(cudaError_t e, const char* what);
+
+#define QCP_CUDA(expr)                                              \
+  do {                                                              \
+    cudaError_t e_ = (expr);                                        \
+    if (e_ != cudaSuccess) return ::qcp::cuda_status(e_, #expr);    \
+  } while (0)
+
+#define QCP_TRY(expr)                    \
+  do {                                   \
+    qcp_status s_ = (expr);              \
+    if (s_ != QCP_OK) return s_;         \
+  } while (0)
+
+// Per-host-thread count of kernel launches made by this library.
+void note_launch(uint32_t k = 1);
+qcp_status check_launch(const char* what);
+
+// ---------------------------------------------------------------------------
+// Device buffers.  A small caching allocator keeps freed buffers per device
+// so that repeated query batches do not call cudaMalloc each time.
+// ---------------------------------------------------------------------------
+struct DevPool {
+  std::mutex mu;
+  std::vector<std::pair<size_t, void*>> free_list;  // (bytes, ptr) ready for reuse
+  std::vector<std::pair<void*, size_t>> sizes;      // every live allocation's size
+  size_t cached_bytes = 0;
+  qcp_status get(size_t bytes, void** out);
+  void put(size_t bytes, void* p);
+  void trim();
+};
+
+struct HostPool {  // pinned host memory for results
+  std::mutex mu;
+  std::vector<std::pair<size_t, void*>> free_list;
+  std::vector<std::pair<void*, size_t>> sizes;
+  qcp_status get(size_t bytes, void** out);
+  void put(size_t bytes, void* p);
+  void trim();
+};
+
+template <class T>
+struct DevArray {
+  T* ptr = nullptr;
+  size_t cap = 0;  // elements
+};
+
+// Scratch for one query call.  Reused across calls through the index's
+// workspace list (one workspace per concurrently running call).
+struct Workspace {
+  float* boxes = nullptr;
+  size_t boxes_cap = 0;          // floats
+  uint2* items[2] = {nullptr, nullptr};
+  size_t items_cap = 0;          // (query, node) items per buffer
+  uint32_t* item_hits = nullptr; // per level-1 item hit counts
+  size_t item_hits_cap = 0;
+  uint64_t* qcount = nullptr;    // per-query counts, q
+  uint64_t* qcursor = nullptr;   // per-query write cursors, q
+  uint64_t* offsets = nullptr;   // q + 1, from the index's pool
+  size_t offsets_cap = 0;
+  size_t q_cap = 0;
+  int32_t* out_ids = nullptr;    // unsorted then sorted ids
+  int32_t* tmp_ids = nullptr;    // segmented-sort ping-pong buffer
+  size_t out_cap = 0;            // ids
+  // segmented sort job lists
+  uint4* jobs[2] = {nullptr, nullptr};
+  size_t jobs_cap = 0;
+  uint32_t* seg_hist = nullptr;  // MSD tile -> job map
+  size_t seg_hist_cap = 0;
+  uint32_t* ctr = nullptr;       // device counters (see kCtr*)
+  uint32_t* h_ctr = nullptr;     // pinned mirror of ctr
+  uint64_t* h_total = nullptr;   // pinned total-hits readback
+  // work counters (kStat* slots) and phase events of the current call
+  unsigned long long* d_stats = nullptr;
+  unsigned long long* h_stats = nullptr;
+  cudaEvent_t ev[8] = {};
+  bool timing = false;
+  uint32_t sort_small_jobs = 0, sort_msd_jobs = 0;
+};
+
+// Slots of Workspace::d_stats.
+enum StatSlot : uint32_t {
+  kStatCovered = 0,     // covered leaves
+  kStatPartial = 1,     // partially covered leaves (objects tested)
+  kStatObjCovered = 2,  // objects in covered leaves
+  kStatLevel0 = 8,      // frontier items of level l at kStatLevel0 + l
+  kStatCount = 24
+};
+
+// Phase events of Workspace::ev.
+enum EvSlot : int { kEvStart = 0, kEvExpand = 1, kEvCount = 2, kEvScan = 3, kEvWrite = 4, kEvSort = 5 };
+
+inline void mark(Workspace* ws, int slot, cudaStream_t s) {
+  if (ws->timing) cudaEventRecord(ws->ev[slot], s);
+}
+
+// Slots of Workspace::ctr.
+enum CtrSlot : uint32_t {
+  kCtrFrontier0 = 0,  // items in items[0]
+  kCtrFrontier1 = 1,  // items in items[1]
+  kCtrWork = 2,       // dynamic work fetch counter
+  kCtrOverflow = 3,   // nonzero: a capacity was exceeded
+  kCtrNeedItems = 4,  // items needed when the frontier overflowed
+  kCtrJobs0 = 5,      // segmented-sort job list sizes
+  kCtrJobs1 = 6,
+  kCtrSmall = 7,      // small-segment job count
+  kCtrWork2 = 8,
+  kCtrCount = 16
+};
+
+}  // namespace qcp
+
+struct qcp_index {
+  int device = 0;
+  uint64_t n = 0;
+  uint32_t dims = 0, is_rect = 0, fanout = 128, levels = 0;
+  uint32_t key_mode = 0, key_bits = 0;
+  uint32_t ncoord = 0;                // dims (points) or 2*dims (rects)
+  uint64_t npad = 0;                  // n rounded up to a multiple of fanout
+  uint64_t level_nodes[qcp::kMaxLevels] = {0};
+  uint64_t level_pad[qcp::kMaxLevels] = {0};
+  float* coords = nullptr;            // [ncoord][npad], sorted order
+  int32_t* ids = nullptr;             // [npad] input id of each sorted position
+  uint64_t* keys = nullptr;           // [n] sorted keys
+  float* mbr[qcp::kMaxLevels] = {nullptr};  // per level [2*dims][level_pad]
+  uint64_t device_bytes = 0;
+
+  qcp::DevPool pool;
+  std::mutex ws_mu;
+  std::vector<qcp::Workspace*> ws_free;
+  std::vector<qcp::Workspace*> ws_all;
+};
+
+namespace qcp {
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+
+// Overlap of a query box with an entry [lo, hi] in every dimension:
+// !(q.lo > e.hi || q.hi < e.lo), the predicate of src/node/node_soa.cpp:94-113.
+__device__ __forceinline__ bool overlaps1(float qlo, float qhi, float lo, float hi) {
+  return !(qlo > hi || qhi < lo);
+}
+// Entry [lo, hi] lies inside the query box in one dimension.  Only used to
+// skip the per-entry test of leaves whose MBR is covered by the query: every
+// finite entry inside such an MBR passes overlaps1.
+__device__ __forceinline__ bool inside1(float qlo, float qhi, float lo, float hi) {
+  return qlo <= lo && hi <= qhi;
+}
+
+__host__ __device__ __forceinline__ uint64_t low_ones64(uint32_t k) {
+  return k >= 64 ? ~0ull : ((1ull << k) - 1ull);
+}
+
+// Hilbert index of integer coordinates, the algorithm of
+// HilbertMapper::MappingIntoSingle (src/mapper/hilbert_mapper.cpp:25-64) and
+// hilbert_macro.h:4-22, written in unsigned 64-bit arithmetic.
+__host__ __device__ inline uint64_t hilbert_index(uint32_t dims, uint32_t bits, const int64_t* coord) {
+  if (dims <= 1) return (uint64_t)coord[0];
+  const uint32_t total = dims * bits;
+  uint64_t packed = 0;
+  for (int d = (int)dims - 1; d >= 0; --d) {
+    packed = (packed << bits) | (uint64_t)coord[d];
+  }
+  // transpose: level b holds bit b of every coordinate (coordinate d at bit d)
+  uint64_t t = 0;
+  for (uint32_t b = 0; b < bits; ++b) {
+    for (uint32_t d = 0; d < dims; ++d) {
+      t |= ((packed >> (d * bits + b)) & 1ull) << (b * dims + d);
+    }
+  }
+  uint64_t index;
+  if (bits > 1) {
+    const uint64_t nd_ones = low_ones64(dims);
+    const uint64_t nd1_ones = nd_ones >> 1;
+    uint64_t level_low = 0;
+    for (uint32_t b = 0; b < bits; ++b) level_low |= 1ull << (b * dims);
+    t ^= t >> dims;
+    index = 0;
+    uint32_t rot = 0;
+    uint64_t flip = 0;
+    for (int lvl = (int)bits - 1; lvl >= 0; --lvl) {
+      uint64_t g = ((t >> (lvl * dims)) & nd_ones) ^ flip;
+      if (rot) g = ((g >> rot) | (g << (dims - rot))) & nd_ones;
+      index = (index << dims) | g;
+      flip = 1ull << rot;
+      uint64_t low = g & (0ull - g) & nd1_ones;
+      while (low) {
+        low >>= 1;
+        ++rot;
+      }
+      if (++rot >= dims) rot -= dims;
+    }
+    index ^= level_low >> 1;
+  } else {
+    index = t;
+  }
+  for (uint32_t s = 1; s < total; s *= 2) index ^= index >> s;
+  return index & low_ones64(total);
+}
+
+// ---------------------------------------------------------------------------
+// Kernel launchers (defined in the .cu files)
+// ---------------------------------------------------------------------------
+int num_sms();
+
+// Build
+qcp_status build_keys(const float* objs, uint64_t n, uint32_t dims, uint32_t is_rect,
+                      uint32_t key_mode, uint32_t key_bits, uint64_t* keys, uint32_t* vals,
+                      cudaStream_t s);
+qcp_status radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp,
+                            uint64_t n, uint32_t key_bits, DevPool& pool, cudaStream_t s,
+                            bool* result_in_tmp);
+qcp_status build_pack(qcp_index* ix, const float* objs, const uint32_t* perm, cudaStream_t s,
+                      uint32_t* d_bad);
+qcp_status build_levels(qcp_index* ix, cudaStream_t s);
+
+// Query
+qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_only, bool sort,
+                       cudaStream_t s);
+qcp_status run_plain(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_only, bool sort,
+                     cudaStream_t s);
+qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t s);
+qcp_status exclusive_scan_counts(const uint64_t* counts, uint64_t* offsets, uint32_t q,
+                                 DevPool& pool, cudaStream_t s);
+template <class T>
+qcp_status exclusive_scan(const T* in, T* out, uint64_t n, T* grand_total, DevPool& pool,
+                          cudaStream_t s);
+
+}  // namespace qcp

@@ -1,0 +1,584 @@
+// Range-search traversal kernels.
+//
+// Batched pipeline (QCP_ALGO_BATCHED), for the whole query batch at once:
+//   1. k_expand, once per level above the leaves' parents: every
+//      (query, node) item of level l becomes the (query, child) items of the
+//      children whose MBR overlaps the query (warp per item, ballot
+//      compaction, one atomic per warp).
+//   2. k_leafscan<COUNT>: every (query, level-1 node) item is fetched
+//      dynamically by a warp from a device work counter; the warp tests the
+//      node's leaf MBRs, counts leaves whose MBR lies inside the query box
+//      without touching their objects, and tests the objects of the other
+//      overlapping leaves with 128-bit coalesced loads.
+//   3. exclusive scan of the per-query counts -> CSR offsets.
+//   4. k_leafscan<WRITE>: the same items again; each warp reserves its
+//      item's slice of the query's output with one atomic and writes ids
+//      (whole id runs for covered leaves, ballot-compacted ids otherwise).
+//   5. per-query sort of the ids (qcp_segsort.cu).
+//
+// Plain traversal (QCP_ALGO_PLAIN): k_mprs, one query per CUDA block,
+// restart scanning + parent check as the reference's
+// global_RestartScanning_and_ParentCheck (src/tree/mphr.cpp:303-438) does,
+// over the implicit node layout, run twice (count, then write).
+//
+// The hit predicate everywhere is the reference's closed-interval test
+// (src/node/node_soa.cpp:94-113).
+#include <cfloat>
+
+#include "qcp_internal.cuh"
+
+namespace qcp {
+
+namespace {
+
+struct TreeView {
+  const float* coords;
+  const int32_t* ids;
+  uint64_t n, npad;
+  uint32_t fanout, levels;
+  const float* mbr[kMaxLevels];
+  uint64_t nodes[kMaxLevels];
+  uint64_t pad[kMaxLevels];
+};
+
+TreeView view_of(const qcp_index* ix) {
+  TreeView v;
+  v.coords = ix->coords;
+  v.ids = ix->ids;
+  v.n = ix->n;
+  v.npad = ix->npad;
+  v.fanout = ix->fanout;
+  v.levels = ix->levels;
+  for (int l = 0; l < kMaxLevels; ++l) {
+    v.mbr[l] = ix->mbr[l];
+    v.nodes[l] = ix->level_nodes[l];
+    v.pad[l] = ix->level_pad[l];
+  }
+  return v;
+}
+
+template <int D>
+struct Box {
+  float lo[D], hi[D];
+};
+
+template <int D>
+__device__ __forceinline__ Box<D> load_box(const float* boxes, uint32_t q) {
+  Box<D> b;
+  const float* p = boxes + (uint64_t)q * 2 * D;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    b.lo[d] = __ldg(p + d);
+    b.hi[d] = __ldg(p + D + d);
+  }
+  return b;
+}
+
+// MBR overlap / containment of node c of a level.
+template <int D>
+__device__ __forceinline__ void test_node(const Box<D>& b, const float* mbr, uint64_t pad, uint64_t c,
+                                          bool& ov, bool& in) {
+  ov = true;
+  in = true;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const float lo = __ldg(mbr + (uint64_t)d * pad + c);
+    const float hi = __ldg(mbr + (uint64_t)(D + d) * pad + c);
+    ov &= overlaps1(b.lo[d], b.hi[d], lo, hi);
+    in &= inside1(b.lo[d], b.hi[d], lo, hi);
+  }
+}
+
+// Hit mask of 4 consecutive objects starting at position p (p % 4 == 0).
+template <int D, bool RECT>
+__device__ __forceinline__ uint32_t test4(const Box<D>& b, const float* coords, uint64_t npad, uint64_t p,
+                                          uint64_t n) {
+  uint32_t m = 0xfu;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const float4 lo = __ldg(reinterpret_cast<const float4*>(coords + (uint64_t)d * npad + p));
+    float4 hi = lo;
+    if (RECT) hi = __ldg(reinterpret_cast<const float4*>(coords + (uint64_t)(D + d) * npad + p));
+    m &= (overlaps1(b.lo[d], b.hi[d], lo.x, hi.x) ? 1u : 0u) | (overlaps1(b.lo[d], b.hi[d], lo.y, hi.y) ? 2u : 0u) |
+         (overlaps1(b.lo[d], b.hi[d], lo.z, hi.z) ? 4u : 0u) | (overlaps1(b.lo[d], b.hi[d], lo.w, hi.w) ? 8u : 0u);
+  }
+  // objects past n (padding of the last leaf) never hit
+  if (p + 4 > n) {
+    const uint64_t valid = (n > p) ? (n - p) : 0;
+    m &= (1u << valid) - 1u;
+  }
+  return m;
+}
+
+__device__ __forceinline__ uint32_t lane_lt_mask() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ uint32_t warp_excl_sum(uint32_t v, uint32_t* total) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  *total = __shfl_sync(0xffffffffu, x, 31);
+  return x - v;
+}
+
+// ---------------------------------------------------------------------------
+// Batched pipeline kernels
+// ---------------------------------------------------------------------------
+__global__ void k_init_items(uint2* items, uint32_t q, uint32_t node, uint32_t* count) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < q; i += gridDim.x * blockDim.x)
+    items[i] = make_uint2(i, node);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *count = q;
+}
+
+template <int D>
+__global__ void __launch_bounds__(256) k_expand(const float* __restrict__ boxes,
+                                                const uint2* __restrict__ in,
+                                                const uint32_t* __restrict__ in_count,
+                                                uint2* __restrict__ out, uint32_t* out_count,
+                                                uint64_t out_cap, const float* __restrict__ child_mbr,
+                                                uint64_t nchild, uint64_t child_pad, uint32_t fanout,
+                                                uint32_t* overflow, uint32_t* need) {
+  const uint32_t lane = threadIdx.x & 31;
+  // the counter keeps counting past the capacity when a level overflowed
+  const uint32_t nin = (uint32_t)min((uint64_t)*in_count, out_cap);
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nin; i += warps) {
+    const uint2 it = in[i];
+    const Box<D> b = load_box<D>(boxes, it.x);
+    const uint64_t c0 = (uint64_t)it.y * fanout;
+    const uint64_t c1 = (c0 + fanout < nchild) ? c0 + fanout : nchild;
+    for (uint64_t cb = c0; cb < c1; cb += 32) {
+      const uint64_t c = cb + lane;
+      bool ov = false, in_ = false;
+      if (c < c1) test_node<D>(b, child_mbr, child_pad, c, ov, in_);
+      const uint32_t m = __ballot_sync(0xffffffffu, ov);
+      if (!m) continue;
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(out_count, (uint32_t)__popc(m));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (ov) {
+        const uint64_t pos = (uint64_t)base + __popc(m & lane_lt_mask());
+        if (pos < out_cap) {
+          out[pos] = make_uint2(it.x, (uint32_t)c);
+        } else {
+          atomicOr(overflow, 1u);
+        }
+      }
+      if (lane == 0 && (uint64_t)base + __popc(m) > out_cap) atomicMax(need, base + __popc(m));
+    }
+  }
+}
+
+enum { kCount = 0, kWrite = 1 };
+
+// Warp per (query, level-1 node) item.  COUNT: item_hits[i] and qcount[q].
+// WRITE: ids at out[offsets[q] + reserved slice].
+template <int D, bool RECT, int MODE>
+__global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __restrict__ boxes,
+                                                  const uint2* __restrict__ items,
+                                                  const uint32_t* __restrict__ item_count,
+                                                  uint32_t* work, uint32_t* __restrict__ item_hits,
+                                                  unsigned long long* qcount,
+                                                  const unsigned long long* __restrict__ offsets,
+                                                  unsigned long long* qcursor,
+                                                  int32_t* __restrict__ out, uint64_t item_cap,
+                                                  unsigned long long* stats) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nitems = (uint32_t)min((uint64_t)*item_count, item_cap);
+  const uint32_t F = t.fanout;
+  const float* lmbr = t.mbr[0];
+  const uint64_t lpad = t.pad[0];
+  const uint64_t nleaves = t.nodes[0];
+  for (;;) {
+    uint32_t i = 0;
+    if (lane == 0) i = atomicAdd(work, 1u);
+    i = __shfl_sync(0xffffffffu, i, 0);
+    if (i >= nitems) break;
+    const uint2 it = items[i];
+    const Box<D> b = load_box<D>(boxes, it.x);
+    uint64_t wpos = 0;
+    if (MODE == kWrite) {
+      const uint32_t mine = item_hits[i];
+      if (mine == 0) continue;
+      if (lane == 0) wpos = offsets[it.x] + atomicAdd(qcursor + it.x, (unsigned long long)mine);
+      wpos = __shfl_sync(0xffffffffu, wpos, 0);
+    }
+    uint32_t hits = 0;  // per lane (count mode)
+    uint32_t n_cov = 0, n_part = 0, o_cov = 0;  // per lane work counters (count mode)
+    const uint64_t l0 = (uint64_t)it.y * F;
+    const uint64_t l1 = (l0 + F < nleaves) ? l0 + F : nleaves;
+    for (uint64_t lb = l0; lb < l1; lb += 32) {
+      const uint64_t leaf = lb + lane;
+      bool ov = false, in_ = false;
+      if (leaf < l1) test_node<D>(b, lmbr, lpad, leaf, ov, in_);
+      const uint32_t mov = __ballot_sync(0xffffffffu, ov);
+      const uint32_t min_ = __ballot_sync(0xffffffffu, in_ && ov);
+      if (!mov) continue;
+      // leaves whose MBR lies inside the query: every object is a hit
+      if (MODE == kCount) {
+        if (in_ && ov) {
+          const uint64_t e0 = leaf * F;
+          const uint64_t e1 = (e0 + F < t.n) ? e0 + F : t.n;
+          hits += (uint32_t)(e1 - e0);
+          o_cov += (uint32_t)(e1 - e0);
+          ++n_cov;
+        } else if (ov) {
+          ++n_part;
+        }
+      } else {
+        uint32_t m = min_;
+        while (m) {
+          // a run of consecutive covered leaves is one contiguous id range
+          const int s = __ffs(m) - 1;
+          const uint32_t shifted = ~(m >> s);
+          const int len = shifted ? (__ffs(shifted) - 1) : (32 - s);
+          m &= ~((len >= 32 ? 0xffffffffu : ((1u << len) - 1u)) << s);
+          const uint64_t e0 = (lb + s) * F;
+          uint64_t e1 = (lb + s + len) * F;
+          if (e1 > t.n) e1 = t.n;
+          const int32_t* src = t.ids + e0;
+          const uint64_t cnt = e1 - e0;
+          for (uint64_t j = lane; j < cnt; j += 32) out[wpos + j] = __ldg(src + j);
+          wpos += cnt;
+        }
+      }
+      // partially covered leaves: test every object
+      uint32_t mp = mov & ~min_;
+      while (mp) {
+        const int s = __ffs(mp) - 1;
+        mp &= mp - 1;
+        const uint64_t e0 = (lb + s) * F;
+        for (uint32_t g0 = 0; g0 < F; g0 += 128) {  // warp-uniform trip count
+          const uint32_t g = g0 + lane * 4;
+          const uint64_t p = e0 + g;
+          const uint32_t hm = (g < F) ? test4<D, RECT>(b, t.coords, t.npad, p, t.n) : 0u;
+          if (MODE == kCount) {
+            hits += __popc(hm);
+          } else {
+            uint32_t tot;
+            const uint32_t ex = warp_excl_sum(__popc(hm), &tot);
+            if (hm) {
+              const int4 idv = __ldg(reinterpret_cast<const int4*>(t.ids + p));
+              uint64_t o = wpos + ex;
+              if (hm & 1u) out[o++] = idv.x;
+              if (hm & 2u) out[o++] = idv.y;
+              if (hm & 4u) out[o++] = idv.z;
+              if (hm & 8u) out[o++] = idv.w;
+            }
+            wpos += tot;
+          }
+        }
+      }
+    }
+    if (MODE == kCount) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        hits += __shfl_xor_sync(0xffffffffu, hits, o);
+        n_cov += __shfl_xor_sync(0xffffffffu, n_cov, o);
+        n_part += __shfl_xor_sync(0xffffffffu, n_part, o);
+        o_cov += __shfl_xor_sync(0xffffffffu, o_cov, o);
+      }
+      if (lane == 0) {
+        item_hits[i] = hits;
+        if (hits) atomicAdd(qcount + it.x, (unsigned long long)hits);
+        if (n_cov) atomicAdd(stats + kStatCovered, (unsigned long long)n_cov);
+        if (n_part) atomicAdd(stats + kStatPartial, (unsigned long long)n_part);
+        if (o_cov) atomicAdd(stats + kStatObjCovered, (unsigned long long)o_cov);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Plain traversal: one query per block, blockDim.x == fanout threads.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t span_of(uint32_t level, uint32_t F) {
+  // objects covered by one node of `level` (level 0 = leaf)
+  uint64_t s = F;
+  for (uint32_t l = 0; l < level; ++l) s *= F;
+  return s;
+}
+
+template <int D, bool RECT, int MODE>
+__global__ void __launch_bounds__(256) k_mprs(TreeView t, const float* __restrict__ boxes, uint32_t nq,
+                                              unsigned long long* __restrict__ counts,
+                                              const unsigned long long* __restrict__ offsets,
+                                              int32_t* __restrict__ out) {
+  __shared__ uint32_t warp_min[8];
+  __shared__ uint32_t warp_cnt[8];
+  __shared__ uint32_t s_leftmost;
+  const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const uint32_t nwarps = blockDim.x >> 5;
+  const uint32_t F = t.fanout;
+  const uint32_t top = t.levels - 1;
+  for (uint32_t q = blockIdx.x; q < nq; q += gridDim.x) {
+    const Box<D> b = load_box<D>(boxes, q);
+    uint64_t written = 0;
+    uint64_t base = (MODE == kWrite) ? offsets[q] : 0;
+    uint64_t visited = 0;  // every object before this position is settled
+    uint32_t level = top;
+    uint64_t node = 0;
+    while (visited < t.n) {
+      // internal phase: leftmost overlapping child not yet visited
+      bool restart = false;
+      while (level > 0) {
+        const uint32_t cl = level - 1;
+        const uint64_t c = node * F + tid;
+        const uint64_t cspan = span_of(cl, F);
+        bool cand = false;
+        if (c < t.nodes[cl]) {
+          uint64_t cend = (c + 1) * cspan;
+          if (cend > t.n) cend = t.n;
+          if (cend > visited) {
+            bool ov, in_;
+            test_node<D>(b, t.mbr[cl], t.pad[cl], c, ov, in_);
+            cand = ov;
+          }
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, cand);
+        if (lane == 0) warp_min[w] = m ? (w * 32 + __ffs(m) - 1) : 0xffffffffu;
+        __syncthreads();
+        if (tid == 0) {
+          uint32_t best = 0xffffffffu;
+          for (uint32_t k = 0; k < nwarps; ++k) best = min(best, warp_min[k]);
+          s_leftmost = best;
+        }
+        __syncthreads();
+        const uint32_t leftmost = s_leftmost;
+        __syncthreads();
+        if (leftmost == 0xffffffffu) {
+          // nothing left under this node: skip it and restart at the root
+          uint64_t nend = (node + 1) * span_of(level, F);
+          if (nend > t.n) nend = t.n;
+          visited = nend;
+          level = top;
+          node = 0;
+          restart = true;
+          break;
+        }
+        node = node * F + leftmost;
+        level = cl;
+      }
+      if (restart) continue;
+      // leaf phase: scan leaves left to right while they hold hits
+      for (;;) {
+        const uint64_t e = node * F + tid;
+        bool hit = false;
+        if (e < t.n) {
+          hit = true;
+#pragma unroll
+          for (int d = 0; d < D; ++d) {
+            const float lo = t.coords[(uint64_t)d * t.npad + e];
+            const float hi = RECT ? t.coords[(uint64_t)(D + d) * t.npad + e] : lo;
+            hit &= overlaps1(b.lo[d], b.hi[d], lo, hi);
+          }
+        }
+        const uint32_t hm = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0) warp_cnt[w] = __popc(hm);
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+        for (uint32_t k = 0; k < nwarps; ++k) {
+          const uint32_t c = warp_cnt[k];
+          if (k < w) before += c;
+          total += c;
+        }
+        if (MODE == kWrite && hit) out[base + written + before + __popc(hm & lane_lt_mask())] = t.ids[e];
+        written += total;
+        __syncthreads();
+        uint64_t lend = (node + 1) * F;
+        if (lend > t.n) lend = t.n;
+        visited = lend;
+        if (lend >= t.n) break;
+        if (total) {
+          ++node;  // next leaf in key order
+        } else {
+          // back to the parent: its remaining children are checked next
+          node /= F;
+          level = 1;
+          break;
+        }
+      }
+      if (level == 0) break;  // reached the last leaf
+      if (top == 0) break;
+    }
+    if (MODE == kCount && tid == 0) counts[q] = written;
+  }
+}
+
+#define QCP_DISPATCH_D(D_, ...)                  \
+  switch (D_) {                                  \
+    case 1: { constexpr int DD = 1; __VA_ARGS__; } break; \
+    case 2: { constexpr int DD = 2; __VA_ARGS__; } break; \
+    case 3: { constexpr int DD = 3; __VA_ARGS__; } break; \
+    case 4: { constexpr int DD = 4; __VA_ARGS__; } break; \
+    case 5: { constexpr int DD = 5; __VA_ARGS__; } break; \
+    case 6: { constexpr int DD = 6; __VA_ARGS__; } break; \
+    case 7: { constexpr int DD = 7; __VA_ARGS__; } break; \
+    case 8: { constexpr int DD = 8; __VA_ARGS__; } break; \
+    default: break;                              \
+  }
+
+template <int D>
+void launch_expand(uint32_t grid, cudaStream_t s, const float* boxes, const uint2* in,
+                   const uint32_t* in_count, uint2* out, uint32_t* out_count, uint64_t cap,
+                   const float* child_mbr, uint64_t nchild, uint64_t child_pad, uint32_t fanout,
+                   uint32_t* overflow, uint32_t* need) {
+  k_expand<D><<<grid, 256, 0, s>>>(boxes, in, in_count, out, out_count, cap, child_mbr, nchild,
+                                   child_pad, fanout, overflow, need);
+}
+
+template <int D, int MODE>
+void launch_leafscan(bool rect, uint32_t grid, cudaStream_t s, const TreeView& t, const float* boxes,
+                     const uint2* items, const uint32_t* item_count, uint32_t* work,
+                     uint32_t* item_hits, uint64_t* qcount, const uint64_t* offsets,
+                     uint64_t* qcursor, int32_t* out, uint64_t item_cap,
+                     unsigned long long* stats) {
+  if (rect)
+    k_leafscan<D, true, MODE><<<grid, 256, 0, s>>>(
+        t, boxes, items, item_count, work, item_hits, (unsigned long long*)qcount,
+        (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap, stats);
+  else
+    k_leafscan<D, false, MODE><<<grid, 256, 0, s>>>(
+        t, boxes, items, item_count, work, item_hits, (unsigned long long*)qcount,
+        (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap, stats);
+}
+
+template <int D, int MODE>
+void launch_mprs(bool rect, uint32_t grid, uint32_t threads, cudaStream_t s, const TreeView& t,
+                 const float* boxes, uint32_t nq, uint64_t* counts, const uint64_t* offsets,
+                 int32_t* out) {
+  if (rect)
+    k_mprs<D, true, MODE><<<grid, threads, 0, s>>>(t, boxes, nq, (unsigned long long*)counts,
+                                                   (const unsigned long long*)offsets, out);
+  else
+    k_mprs<D, false, MODE><<<grid, threads, 0, s>>>(t, boxes, nq, (unsigned long long*)counts,
+                                                    (const unsigned long long*)offsets, out);
+}
+
+}  // namespace
+
+// Grows the workspace buffers a batch of q queries needs before its items
+// are known (items and output grow on demand below).
+qcp_status ws_reserve_queries(qcp_index* ix, Workspace* ws, uint32_t q);
+qcp_status ws_reserve_items(qcp_index* ix, Workspace* ws, size_t items);
+qcp_status ws_reserve_out(qcp_index* ix, Workspace* ws, size_t ids);
+
+qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_only, bool sort,
+                       cudaStream_t s) {
+  const TreeView t = view_of(ix);
+  const uint32_t D = ix->dims;
+  const bool rect = ix->is_rect != 0;
+  const uint32_t sms = (uint32_t)num_sms();
+  const uint32_t grid = sms * 8;  // 8 x 256 threads resident per SM
+  uint32_t* ctr = ws->ctr;
+  // start level: items at level `start` are (query, node) pairs
+  const uint32_t start = (ix->levels >= 2) ? ix->levels - 1 : 1;
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    mark(ws, kEvStart, s);
+    QCP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * kCtrCount, s));
+    QCP_CUDA(cudaMemsetAsync(ws->d_stats, 0, sizeof(unsigned long long) * kStatCount, s));
+    QCP_CUDA(cudaMemsetAsync(ws->qcount, 0, sizeof(uint64_t) * q, s));
+    k_init_items<<<(q + 255) / 256, 256, 0, s>>>(ws->items[0], q, 0, ctr + kCtrFrontier0);
+    note_launch();
+    QCP_CUDA(cudaMemcpyAsync(ws->d_stats + kStatLevel0 + start, ctr + kCtrFrontier0, sizeof(uint32_t),
+                             cudaMemcpyDeviceToDevice, s));
+    int cur = 0;
+    for (uint32_t l = start; l > 1; --l) {
+      const int nxt = cur ^ 1;
+      QCP_CUDA(cudaMemsetAsync(ctr + kCtrFrontier0 + nxt, 0, sizeof(uint32_t), s));
+      QCP_DISPATCH_D(D, launch_expand<DD>(grid, s, ws->boxes, ws->items[cur], ctr + kCtrFrontier0 + cur,
+                                          ws->items[nxt], ctr + kCtrFrontier0 + nxt, ws->items_cap,
+                                          t.mbr[l - 1], t.nodes[l - 1], t.pad[l - 1], t.fanout,
+                                          ctr + kCtrOverflow, ctr + kCtrNeedItems));
+      note_launch();
+      QCP_CUDA(cudaMemcpyAsync(ws->d_stats + kStatLevel0 + (l - 1), ctr + kCtrFrontier0 + nxt,
+                               sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+      cur = nxt;
+    }
+    QCP_TRY(check_launch("k_expand"));
+    mark(ws, kEvExpand, s);
+    // the level-1 items must fit the per-item hit array too
+    QCP_TRY(ws_reserve_items(ix, ws, 0));
+    QCP_DISPATCH_D(D, launch_leafscan<DD, kCount>(rect, grid, s, t, ws->boxes, ws->items[cur],
+                                                  ctr + kCtrFrontier0 + cur, ctr + kCtrWork,
+                                                  ws->item_hits, ws->qcount, nullptr, nullptr, nullptr,
+                                                  ws->items_cap, ws->d_stats));
+    note_launch();
+    QCP_TRY(check_launch("k_leafscan<count>"));
+    mark(ws, kEvCount, s);
+    QCP_TRY(exclusive_scan_counts(ws->qcount, ws->offsets, q, ix->pool, s));
+    mark(ws, kEvScan, s);
+    // one readback: overflow flags, items needed, total hits
+    QCP_CUDA(cudaMemcpyAsync(ws->h_ctr, ctr, sizeof(uint32_t) * kCtrCount, cudaMemcpyDeviceToHost, s));
+    QCP_CUDA(cudaMemcpyAsync(ws->h_total, ws->offsets + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    QCP_CUDA(cudaStreamSynchronize(s));
+    if (ws->h_ctr[kCtrOverflow]) {
+      size_t need = (size_t)ws->h_ctr[kCtrNeedItems];
+      if (need < ws->items_cap * 2) need = ws->items_cap * 2;
+      QCP_TRY(ws_reserve_items(ix, ws, need));
+      continue;
+    }
+    if (counts_only) return QCP_OK;
+    const uint64_t total = *ws->h_total;
+    QCP_TRY(ws_reserve_out(ix, ws, (size_t)total));
+    if (total) {
+      QCP_CUDA(cudaMemsetAsync(ws->qcursor, 0, sizeof(uint64_t) * q, s));
+      QCP_CUDA(cudaMemsetAsync(ctr + kCtrWork, 0, sizeof(uint32_t), s));
+      QCP_DISPATCH_D(D, launch_leafscan<DD, kWrite>(rect, grid, s, t, ws->boxes, ws->items[cur],
+                                                    ctr + kCtrFrontier0 + cur, ctr + kCtrWork,
+                                                    ws->item_hits, nullptr, ws->offsets, ws->qcursor,
+                                                    ws->out_ids, ws->items_cap, ws->d_stats));
+      note_launch();
+      QCP_TRY(check_launch("k_leafscan<write>"));
+      mark(ws, kEvWrite, s);
+      if (sort) QCP_TRY(segmented_sort(ix, ws, q, s));
+      mark(ws, kEvSort, s);
+    }
+    return QCP_OK;
+  }
+  set_error("query frontier did not fit after repeated growth");
+  return QCP_ERR_OOM;
+}
+
+qcp_status run_plain(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_only, bool sort,
+                     cudaStream_t s) {
+  const TreeView t = view_of(ix);
+  const uint32_t D = ix->dims;
+  const bool rect = ix->is_rect != 0;
+  const uint32_t threads = ix->fanout;
+  uint32_t grid = q ? q : 1;
+  if (grid > (uint32_t)num_sms() * 64) grid = (uint32_t)num_sms() * 64;
+  mark(ws, kEvStart, s);
+  mark(ws, kEvExpand, s);
+  QCP_DISPATCH_D(D, launch_mprs<DD, kCount>(rect, grid, threads, s, t, ws->boxes, q, ws->qcount,
+                                            nullptr, nullptr));
+  note_launch();
+  QCP_TRY(check_launch("k_mprs<count>"));
+  mark(ws, kEvCount, s);
+  QCP_TRY(exclusive_scan_counts(ws->qcount, ws->offsets, q, ix->pool, s));
+  mark(ws, kEvScan, s);
+  QCP_CUDA(cudaMemcpyAsync(ws->h_total, ws->offsets + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  QCP_CUDA(cudaStreamSynchronize(s));
+  if (counts_only) return QCP_OK;
+  const uint64_t total = *ws->h_total;
+  QCP_TRY(ws_reserve_out(ix, ws, (size_t)total));
+  if (total) {
+    QCP_DISPATCH_D(D, launch_mprs<DD, kWrite>(rect, grid, threads, s, t, ws->boxes, q, nullptr,
+                                              ws->offsets, ws->out_ids));
+    note_launch();
+    QCP_TRY(check_launch("k_mprs<write>"));
+    mark(ws, kEvWrite, s);
+    if (sort) QCP_TRY(segmented_sort(ix, ws, q, s));
+    mark(ws, kEvSort, s);
+  }
+  return QCP_OK;
+}
+
+}  // namespace qcp

@@ -1,0 +1,182 @@
+"""Parity of the CUDA path with the oracle (and through it with the
+reference's own counts), called through the C ABI.  Needs a GPU.
+
+Bar: per-query sorted id lists bit-exact (integer/index output of FP32
+closed-interval compares, no tolerance)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import assert_same_hits, golden
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["u3", "g3", "small3", "ragged3", "dup3", "u2", "p8"]
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("algo", ["batched", "plain"])
+def test_golden_cases_exact(qcp, oracle, cases, name, algo):
+    objs, boxes, dims = cases.COUNT_CASES[name]()
+    ref_counts = golden(f"counts_{name}.npz")["counts"].astype(np.uint64)
+    want_offs, want_ids = oracle.ids(objs, dims, False, boxes)
+    assert np.array_equal(np.diff(want_offs), ref_counts)
+    with qcp.Index.build(objs) as ix:
+        res = ix.search(boxes, algo=algo)
+        assert_same_hits(res.offsets, res.ids, want_offs, want_ids, boxes)
+        assert np.array_equal(ix.counts(boxes, algo=algo), ref_counts)
+
+
+@pytest.mark.parametrize("fanout", [32, 64, 128, 192, 256])
+def test_fanouts(qcp, oracle, cases, fanout):
+    objs, boxes, dims = cases.COUNT_CASES["g3"]()
+    want_offs, want_ids = oracle.ids(objs, dims, False, boxes)
+    with qcp.Index.build(objs, fanout=fanout) as ix:
+        info = ix.info()
+        assert info["level_nodes"] == oracle.level_sizes(len(objs), fanout)
+        for algo in ["batched", "plain"]:
+            res = ix.search(boxes, algo=algo)
+            assert_same_hits(res.offsets, res.ids, want_offs, want_ids, boxes)
+
+
+@pytest.mark.parametrize("n", [1, 2, 31, 32, 33, 127, 128, 129, 4095, 16384, 16385])
+def test_small_and_ragged_sizes(qcp, oracle, n):
+    rng = np.random.default_rng(n)
+    objs = rng.random((n, 3), dtype=np.float32)
+    c = rng.random((50, 3), dtype=np.float32)
+    s = rng.uniform(0.05, 0.8, (50, 1)).astype(np.float32)
+    boxes = np.concatenate([c - s / 2, c + s / 2], 1).astype(np.float32)
+    boxes = np.concatenate([boxes, np.array([[-1, -1, -1, 2, 2, 2], [2, 2, 2, 3, 3, 3]], np.float32)])
+    want_offs, want_ids = oracle.ids(objs, 3, False, boxes)
+    with qcp.Index.build(objs, fanout=32) as ix:
+        for algo in ["batched", "plain"]:
+            res = ix.search(boxes, algo=algo)
+            assert_same_hits(res.offsets, res.ids, want_offs, want_ids, boxes)
+
+
+def test_empty_query_batch(qcp, cases):
+    objs, _, _ = cases.COUNT_CASES["u3"]()
+    with qcp.Index.build(objs) as ix:
+        res = ix.search(np.zeros((0, 6), np.float32))
+        assert res.total_hits == 0 and len(res.offsets) == 1
+
+
+def test_config1_exact(qcp, oracle, workloads):
+    """1 M uniform points, 1 000 cubes of side 0.0464 (~100 hits each)."""
+    w = workloads.config1()
+    want_offs, want_ids = oracle.ids(w.objs, 3, False, w.boxes, threads=16)
+    with qcp.Index.build(w.objs, fanout=w.fanout) as ix:
+        for algo in ["batched", "plain"]:
+            res = ix.search(w.boxes, algo=algo)
+            assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
+
+
+def test_unsorted_gives_same_sets(qcp, oracle, cases):
+    objs, boxes, dims = cases.COUNT_CASES["g3"]()
+    want_offs, want_ids = oracle.ids(objs, dims, False, boxes)
+    with qcp.Index.build(objs) as ix:
+        res = ix.search(boxes, sort=False)
+        assert np.array_equal(res.offsets, want_offs)
+        for i in range(len(boxes)):
+            assert np.array_equal(np.sort(res.hits(i)), want_ids[want_offs[i]:want_offs[i + 1]])
+
+
+class _DeviceArray:
+    """A non-owning view of library-owned device memory for torch.as_tensor."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (int(ptr), True),
+                                         "version": 3}
+
+
+def test_device_buffers_in_and_out(qcp, oracle, cases):
+    import torch
+    objs, boxes, dims = cases.COUNT_CASES["g3"]()
+    want_offs, want_ids = oracle.ids(objs, dims, False, boxes)
+    d_objs = torch.from_numpy(objs).cuda()
+    d_boxes = torch.from_numpy(boxes).cuda()
+    with qcp.Index.build(d_objs, dims=3, n=len(objs)) as ix:
+        r = ix.search(d_boxes, q=len(boxes), result_mem=qcp.MEM_DEVICE)
+        try:
+            offs = torch.as_tensor(_DeviceArray(r.offsets, len(boxes) + 1, "<u8"), device="cuda")
+            offs = offs.cpu().numpy().astype(np.uint64)
+            ids = torch.as_tensor(_DeviceArray(r.ids, r.total_hits, "<i4"), device="cuda").cpu().numpy()
+        finally:
+            r.release()
+        assert_same_hits(offs, ids, want_offs, want_ids)
+
+
+def test_ref_key_mode_matches_oracle_keys(qcp, oracle, cases):
+    objs, boxes, dims = cases.COUNT_CASES["dup3"]()
+    with qcp.Index.build(objs, key_mode=qcp.KEY_REF) as ix:
+        keys, perm, _ = ix.export()
+        want_keys = oracle.hilbert_keys(objs, 3, False, 20, 0)
+        order = oracle.sort_perm(want_keys)
+        assert np.array_equal(perm, order.astype(np.int32))       # stable order
+        assert np.array_equal(keys, want_keys[order])
+        res = ix.search(boxes)
+        want_offs, want_ids = oracle.ids(objs, dims, False, boxes)
+        assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
+
+
+@pytest.mark.parametrize("dims,bits", [(2, 32), (3, 21), (8, 8)])
+def test_norm_keys_and_mbrs_match_oracle(qcp, oracle, dims, bits):
+    rng = np.random.default_rng(dims)
+    objs = rng.random((30000, dims), dtype=np.float32)
+    with qcp.Index.build(objs, fanout=64) as ix:
+        keys, perm, _ = ix.export()
+        want = oracle.hilbert_keys(objs, dims, False, bits, 1)
+        order = oracle.sort_perm(want)
+        assert np.array_equal(perm, order.astype(np.int32))
+        assert np.array_equal(keys, want[order])
+        levels = oracle.node_mbrs(objs[order], dims, False, 64)
+        for l, want_mbr in enumerate(levels):
+            _, _, mbr = ix.export(level=l)
+            assert np.array_equal(mbr, want_mbr)
+
+
+def test_rectangles_8d(qcp, oracle):
+    rng = np.random.default_rng(8)
+    lo = rng.random((20000, 8), dtype=np.float32)
+    hi = (lo + rng.exponential(0.05, (20000, 8)).astype(np.float32)).astype(np.float32)
+    objs = np.ascontiguousarray(np.concatenate([lo, hi], 1))
+    c = rng.random((100, 8), dtype=np.float32)
+    s = rng.uniform(0.3, 0.7, (100, 8)).astype(np.float32) / 2
+    boxes = np.concatenate([c - s, c + s], 1).astype(np.float32)
+    want_offs, want_ids = oracle.ids(objs, 8, True, boxes)
+    with qcp.Index.build(objs, is_rect=True) as ix:
+        for algo in ["batched", "plain"]:
+            res = ix.search(boxes, algo=algo)
+            assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
+
+
+def test_save_load_roundtrip(qcp, cases, tmp_path):
+    objs, boxes, dims = cases.COUNT_CASES["u3"]()
+    with qcp.Index.build(objs) as ix:
+        a = ix.search(boxes)
+        ix.save(tmp_path / "ix.qcp")
+    with qcp.Index.load(tmp_path / "ix.qcp") as ix2:
+        b = ix2.search(boxes)
+    assert np.array_equal(a.offsets, b.offsets) and np.array_equal(a.ids, b.ids)
+
+
+def test_nonfinite_objects_rejected(qcp):
+    objs = np.random.default_rng(0).random((1000, 3), dtype=np.float32)
+    objs[10, 1] = np.nan
+    with pytest.raises(qcp.QcpError) as e:
+        qcp.Index.build(objs)
+    assert e.value.status == 1
+
+
+def test_repeated_calls_reuse_buffers(qcp, oracle, cases):
+    objs, boxes, dims = cases.COUNT_CASES["g3"]()
+    want_offs, want_ids = oracle.ids(objs, dims, False, boxes)
+    with qcp.Index.build(objs) as ix:
+        for k in range(3):
+            sub = boxes[k::3]
+            res = ix.search(sub)
+            o, i = oracle.ids(objs, dims, False, sub)
+            assert_same_hits(res.offsets, res.ids, o, i)
+        res = ix.search(boxes)
+        assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
