@@ -283,17 +283,18 @@ class Index:
                    else np.zeros(0, np.int32))
             return SearchResult(offs, ids, int(r.total_hits), MEM_HOST, raw=r)
         if result_mem == MEM_HOST:
+            total = int(r.total_hits)
             try:
                 offs = np.ctypeslib.as_array(ctypes.cast(r.offsets, ctypes.POINTER(ctypes.c_uint64)),
                                              shape=(nq + 1,)).copy()
-                if r.total_hits:
+                if total:
                     ids = np.ctypeslib.as_array(ctypes.cast(r.ids, ctypes.POINTER(ctypes.c_int32)),
-                                                shape=(int(r.total_hits),)).copy()
+                                                shape=(total,)).copy()
                 else:
                     ids = np.zeros(0, np.int32)
             finally:
                 lib.qcp_result_release(ctypes.byref(r))
-            return SearchResult(offs, ids, int(r.total_hits), MEM_HOST)
+            return SearchResult(offs, ids, total, MEM_HOST)
         return SearchResult(r.offsets, r.ids, int(r.total_hits), MEM_DEVICE, raw=r)
 
     def counts(self, boxes, algo="batched", q: int | None = None, stream: int = 0) -> np.ndarray:

@@ -3,37 +3,46 @@
 // The reference returns hit counts only; this library returns every query's
 // hits as ascending input ids.  The traversal writes each query's ids in
 // arbitrary order into its CSR slice; this file sorts every slice in place.
-// Ids of one slice are distinct and lie in [0, n), so only the low
-// `idbits` = ceil(log2 n) bits carry order.
+// The ids of one slice are distinct and lie in [0, n), so only the low
+// `idbits` = ceil(log2 n) bits carry order, and a slice can be sorted by
+// setting one bit per id in a bitmap and reading the bitmap back in order.
 //
-//   slice <= kCap ids:  one CTA loads it into shared memory and runs a stable
-//                       LSD radix sort with 8-bit digits (warp-match ranks),
-//                       then writes it back.
-//   slice >  kCap ids:  MSD rounds.  A round buckets the slice by the next 8
-//                       bits below `hibit` (tile histograms -> per-slice
-//                       bucket bases -> unordered scatter into the other
-//                       buffer); every bucket of <= kCap ids is then sorted
-//                       in shared memory into the output buffer, larger
-//                       buckets go to the next round.  Distinct ids with at
-//                       most 12 significant bits left always fit kCap, so
-//                       31-bit ids need at most three rounds.
+//   slice <= kSmallCap ids   one 512-thread CTA sorts it in shared memory
+//                            (stable LSD radix, 8-bit digits, warp-match
+//                            ranks).
+//   larger slices            1. window partition: ids are bucketed by
+//                               id >> kWinBits into G = 2^(idbits-kWinBits)
+//                               windows (tile histograms -> per-slice window
+//                               bases -> each tile regrouped by window in
+//                               shared memory and written as contiguous runs
+//                               into the scratch buffer);
+//                            2. one CTA per (slice, window): a window of
+//                               W = 2^kWinBits possible ids is a 64 KiB bitmap
+//                               in shared memory; dense windows set a bit per
+//                               id and compact the bitmap in order, sparse
+//                               windows (fewer than one id per 8 bitmap
+//                               words) use the radix sort instead.
+//                            With idbits <= kWinBits there is one window and
+//                            step 1 is skipped (the slice is sorted in place).
 #include "qcp_internal.cuh"
 
 namespace qcp {
 
 namespace {
 
-constexpr int SS_THREADS = 256;
-constexpr int SS_WARPS = SS_THREADS / 32;
-constexpr uint32_t kCap = 4096;
-constexpr uint32_t SS_PER_WARP = kCap / SS_WARPS;  // 512
-constexpr uint32_t SS_ROUNDS = SS_PER_WARP / 32;   // 16
-constexpr uint32_t kTile = 4096;
+constexpr uint32_t kSmallCap = 8192;   // ids sorted by one CTA
+constexpr uint32_t kSortThreads = 512;
+constexpr uint32_t kSortWarps = kSortThreads / 32;
+constexpr uint32_t kRounds = kSmallCap / kSortWarps / 32;  // 16 ids per lane
+constexpr uint32_t kWinBits = 19;      // 2^19 ids per window -> 64 KiB bitmap
+constexpr uint32_t kTile = 4096;       // ids per partition tile
+constexpr uint32_t kTileThreads = 256;
+constexpr uint32_t kMaxWindows = 1u << (31 - kWinBits);
 
 struct Job {
   unsigned long long off;
   uint32_t size;
-  uint32_t info;  // bit 0: data in tmp (1) or out (0); bits 8..15: hibit
+  uint32_t pad;
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt_() {
@@ -42,21 +51,31 @@ __device__ __forceinline__ uint32_t lanemask_lt_() {
   return m;
 }
 
-// Stable LSD sort of a[0..n) (n <= kCap) on bits [0, hibit); the result ends
-// in a.  b is scratch of kCap words.
-__device__ void smem_sort(uint32_t* a, uint32_t* b, uint32_t n, uint32_t hibit,
-                          uint32_t (*wcnt)[256], uint32_t* dig_excl, uint32_t* wtot) {
+// Shared memory of the radix sort (placed at the start of dynamic smem).
+struct RadixSmem {
+  uint32_t a[kSmallCap];
+  uint32_t b[kSmallCap];
+  uint32_t wcnt[kSortWarps][256];
+  uint32_t dig_excl[256];
+  uint32_t wtot[kSortWarps];
+};
+
+// Stable LSD sort of s.a[0..n) (n <= kSmallCap) on bits [0, hibit); the
+// result ends in s.a.  Needs blockDim.x == kSortThreads.
+__device__ void radix_sort_smem(RadixSmem& s, uint32_t n, uint32_t hibit) {
   const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const uint32_t passes = (hibit + 7) / 8;
+  uint32_t* a = s.a;
+  uint32_t* b = s.b;
   for (uint32_t p = 0; p < passes; ++p) {
     const uint32_t shift = 8 * p;
-    for (uint32_t i = tid; i < SS_WARPS * 256; i += SS_THREADS) (&wcnt[0][0])[i] = 0;
+    for (uint32_t i = tid; i < kSortWarps * 256; i += kSortThreads) (&s.wcnt[0][0])[i] = 0;
     __syncthreads();
-    uint32_t rank[SS_ROUNDS];
-    uint32_t key[SS_ROUNDS];
+    uint32_t rank[kRounds];
+    uint32_t key[kRounds];
 #pragma unroll
-    for (uint32_t r = 0; r < SS_ROUNDS; ++r) {
-      const uint32_t li = w * SS_PER_WARP + r * 32 + lane;
+    for (uint32_t r = 0; r < kRounds; ++r) {
+      const uint32_t li = (w * kRounds + r) * 32 + lane;
       const bool valid = li < n;
       key[r] = valid ? a[li] : 0u;
       rank[r] = 0;
@@ -64,48 +83,43 @@ __device__ void smem_sort(uint32_t* a, uint32_t* b, uint32_t n, uint32_t hibit,
       if (valid) {
         const uint32_t d = (key[r] >> shift) & 255u;
         const uint32_t peers = __match_any_sync(active, d);
-        const uint32_t prev = wcnt[w][d];
+        const uint32_t prev = s.wcnt[w][d];
         rank[r] = prev + __popc(peers & lanemask_lt_());
         __syncwarp(active);
-        if (lane == (uint32_t)(__ffs(peers) - 1)) wcnt[w][d] = prev + __popc(peers);
+        if (lane == (uint32_t)(__ffs(peers) - 1)) s.wcnt[w][d] = prev + __popc(peers);
         __syncwarp(active);
       }
     }
     __syncthreads();
-    // per digit (thread = digit): exclusive across warps, then across digits
+    // digit d = tid (threads 0..255): exclusive across warps, then digits
     uint32_t run = 0;
-    for (int k = 0; k < SS_WARPS; ++k) {
-      const uint32_t c = wcnt[k][tid];
-      wcnt[k][tid] = run;
-      run += c;
+    if (tid < 256) {
+      for (uint32_t k = 0; k < kSortWarps; ++k) {
+        const uint32_t c = s.wcnt[k][tid];
+        s.wcnt[k][tid] = run;
+        run += c;
+      }
     }
-    // block exclusive scan of run over the 256 digits
     uint32_t x = run;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
       if (lane >= (uint32_t)o) x += y;
     }
-    if (lane == 31) wtot[w] = x;
+    if (lane == 31 && w < 8) s.wtot[w] = x;
     __syncthreads();
-    if (w == 0) {
-      uint32_t t = (lane < SS_WARPS) ? wtot[lane] : 0u;
-#pragma unroll
-      for (int o = 1; o < SS_WARPS; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
-        if (lane >= (uint32_t)o) t += y;
-      }
-      if (lane < SS_WARPS) wtot[lane] = t;
+    if (tid < 256) {
+      uint32_t before = 0;
+      for (uint32_t k = 0; k < w; ++k) before += s.wtot[k];
+      s.dig_excl[tid] = before + x - run;
     }
     __syncthreads();
-    dig_excl[tid] = ((w > 0) ? wtot[w - 1] : 0u) + x - run;
-    __syncthreads();
 #pragma unroll
-    for (uint32_t r = 0; r < SS_ROUNDS; ++r) {
-      const uint32_t li = w * SS_PER_WARP + r * 32 + lane;
+    for (uint32_t r = 0; r < kRounds; ++r) {
+      const uint32_t li = (w * kRounds + r) * 32 + lane;
       if (li < n) {
         const uint32_t d = (key[r] >> shift) & 255u;
-        b[dig_excl[d] + wcnt[w][d] + rank[r]] = key[r];
+        b[s.dig_excl[d] + s.wcnt[w][d] + rank[r]] = key[r];
       }
     }
     __syncthreads();
@@ -113,26 +127,14 @@ __device__ void smem_sort(uint32_t* a, uint32_t* b, uint32_t n, uint32_t hibit,
     a = b;
     b = t;
   }
-  if (passes & 1) {  // result is in the original b: copy back to a
-    for (uint32_t i = tid; i < n; i += SS_THREADS) b[i] = a[i];
+  if (passes & 1) {
+    for (uint32_t i = tid; i < n; i += kSortThreads) b[i] = a[i];  // back into s.a
     __syncthreads();
   }
 }
 
-// Sorts `size` ids from src[off..) into out[off..) (src may equal out).
-__device__ void sort_slice(const int32_t* src, int32_t* out, unsigned long long off, uint32_t size,
-                           uint32_t hibit, uint32_t* sa, uint32_t* sb, uint32_t (*wcnt)[256],
-                           uint32_t* dig_excl, uint32_t* wtot) {
-  for (uint32_t i = threadIdx.x; i < size; i += SS_THREADS) sa[i] = (uint32_t)src[off + i];
-  __syncthreads();
-  if (size > 1) smem_sort(sa, sb, size, hibit, wcnt, dig_excl, wtot);
-  for (uint32_t i = threadIdx.x; i < size; i += SS_THREADS) out[off + i] = (int32_t)sa[i];
-  __syncthreads();
-}
-
-// Splits the queries into small jobs (sorted directly) and big jobs (MSD).
-__global__ void k_classify(const unsigned long long* __restrict__ offsets, uint32_t q, uint32_t idbits,
-                           Job* small, uint32_t* nsmall, Job* big, uint32_t* nbig) {
+__global__ void k_classify(const unsigned long long* __restrict__ offsets, uint32_t q, Job* small,
+                           uint32_t* nsmall, Job* big, uint32_t* nbig) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < q; i += gridDim.x * blockDim.x) {
     const unsigned long long off = offsets[i];
     const unsigned long long sz = offsets[i + 1] - off;
@@ -140,8 +142,8 @@ __global__ void k_classify(const unsigned long long* __restrict__ offsets, uint3
     Job j;
     j.off = off;
     j.size = (uint32_t)sz;
-    j.info = idbits << 8;
-    if (sz <= kCap) {
+    j.pad = 0;
+    if (sz <= kSmallCap) {
       small[atomicAdd(nsmall, 1u)] = j;
     } else {
       big[atomicAdd(nbig, 1u)] = j;
@@ -149,17 +151,18 @@ __global__ void k_classify(const unsigned long long* __restrict__ offsets, uint3
   }
 }
 
-__global__ void __launch_bounds__(SS_THREADS) k_sort_small(const Job* __restrict__ jobs, uint32_t njobs,
-                                                           int32_t* out, int32_t* tmp) {
-  __shared__ uint32_t sa[kCap];
-  __shared__ uint32_t sb[kCap];
-  __shared__ uint32_t wcnt[SS_WARPS][256];
-  __shared__ uint32_t dig_excl[256];
-  __shared__ uint32_t wtot[SS_WARPS];
+// One CTA per small slice: load, radix sort on the low idbits, store.
+__global__ void __launch_bounds__(kSortThreads) k_sort_small(const Job* __restrict__ jobs, uint32_t njobs,
+                                                             int32_t* out, uint32_t idbits) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RadixSmem& s = *reinterpret_cast<RadixSmem*>(smem_raw);
   for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
     const Job jb = jobs[j];
-    const int32_t* src = (jb.info & 1u) ? tmp : out;
-    sort_slice(src, out, jb.off, jb.size, (jb.info >> 8) & 255u, sa, sb, wcnt, dig_excl, wtot);
+    for (uint32_t i = threadIdx.x; i < jb.size; i += kSortThreads) s.a[i] = (uint32_t)out[jb.off + i];
+    __syncthreads();
+    radix_sort_smem(s, jb.size, idbits);
+    for (uint32_t i = threadIdx.x; i < jb.size; i += kSortThreads) out[jb.off + i] = (int32_t)s.a[i];
+    __syncthreads();
   }
 }
 
@@ -176,138 +179,222 @@ __global__ void k_tile_map(const uint32_t* __restrict__ tiles, const uint32_t* _
   }
 }
 
-__device__ __forceinline__ uint32_t msd_digit(uint32_t id, uint32_t hibit) {
-  const uint32_t lo = hibit > 8 ? hibit - 8 : 0;
-  return (id >> lo) & 255u;
-}
-
-__global__ void __launch_bounds__(SS_THREADS) k_msd_hist(const Job* __restrict__ jobs,
-                                                         const uint32_t* __restrict__ map,
-                                                         const uint32_t* __restrict__ tile_off,
-                                                         uint32_t ntiles, const int32_t* out,
-                                                         const int32_t* tmp, uint32_t* hist) {
-  __shared__ uint32_t h[256];
+// Window histogram of every tile -> whist[job][window].
+__global__ void __launch_bounds__(kTileThreads) k_win_hist(const Job* __restrict__ jobs,
+                                                           const uint32_t* __restrict__ map,
+                                                           const uint32_t* __restrict__ tile_off,
+                                                           uint32_t ntiles, const int32_t* __restrict__ src,
+                                                           uint32_t G, uint32_t* whist) {
+  extern __shared__ uint32_t h[];
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    h[threadIdx.x] = 0;
+    for (uint32_t w = threadIdx.x; w < G; w += kTileThreads) h[w] = 0;
     __syncthreads();
     const uint32_t j = map[t];
     const Job jb = jobs[j];
-    const int32_t* src = (jb.info & 1u) ? tmp : out;
-    const uint32_t hibit = (jb.info >> 8) & 255u;
-    const uint32_t k = t - tile_off[j];
-    const uint32_t b0 = k * kTile;
+    const uint32_t b0 = (t - tile_off[j]) * kTile;
     const uint32_t b1 = min(b0 + kTile, jb.size);
-    for (uint32_t i = b0 + threadIdx.x; i < b1; i += SS_THREADS)
-      atomicAdd(&h[msd_digit((uint32_t)src[jb.off + i], hibit)], 1u);
+    for (uint32_t i = b0 + threadIdx.x; i < b1; i += kTileThreads)
+      atomicAdd(&h[(uint32_t)src[jb.off + i] >> kWinBits], 1u);
     __syncthreads();
-    if (h[threadIdx.x]) atomicAdd(&hist[(size_t)j * 256 + threadIdx.x], h[threadIdx.x]);
+    for (uint32_t w = threadIdx.x; w < G; w += kTileThreads)
+      if (h[w]) atomicAdd(&whist[(size_t)j * G + w], h[w]);
     __syncthreads();
   }
 }
 
-// Per job: exclusive scan of its 256 bucket counts -> absolute bucket bases
-// (base) and write cursors (cursor).
-__global__ void __launch_bounds__(SS_THREADS) k_msd_scan(const Job* __restrict__ jobs, uint32_t njobs,
-                                                         const uint32_t* __restrict__ hist,
-                                                         unsigned long long* base,
-                                                         unsigned long long* cursor) {
-  __shared__ uint32_t wtot[SS_WARPS];
+// Per job: exclusive scan over its G window counts -> absolute bases and cursors.
+__global__ void __launch_bounds__(kTileThreads) k_win_scan(const Job* __restrict__ jobs, uint32_t njobs,
+                                                           uint32_t G, const uint32_t* __restrict__ whist,
+                                                           unsigned long long* wbase,
+                                                           unsigned long long* wcur) {
+  __shared__ uint32_t wt[kTileThreads / 32];
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t per = (G + kTileThreads - 1) / kTileThreads;  // consecutive windows per thread
   for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
-    const uint32_t c = hist[(size_t)j * 256 + threadIdx.x];
-    uint32_t x = c;
+    const size_t base = (size_t)j * G;
+    const uint32_t w0 = threadIdx.x * per;
+    uint32_t s = 0;
+    for (uint32_t k = 0; k < per; ++k)
+      if (w0 + k < G) s += whist[base + w0 + k];
+    uint32_t x = s;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
       if (lane >= (uint32_t)o) x += y;
     }
-    if (lane == 31) wtot[w] = x;
+    if (lane == 31) wt[w] = x;
     __syncthreads();
     uint32_t before = 0;
-    for (uint32_t k = 0; k < w; ++k) before += wtot[k];
-    const unsigned long long b = jobs[j].off + before + x - c;
-    base[(size_t)j * 256 + threadIdx.x] = b;
-    cursor[(size_t)j * 256 + threadIdx.x] = b;
+    for (uint32_t k = 0; k < w; ++k) before += wt[k];
+    unsigned long long run = jobs[j].off + before + x - s;
+    for (uint32_t k = 0; k < per; ++k) {
+      if (w0 + k < G) {
+        wbase[base + w0 + k] = run;
+        wcur[base + w0 + k] = run;
+        run += whist[base + w0 + k];
+      }
+    }
     __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(SS_THREADS) k_msd_scatter(const Job* __restrict__ jobs,
-                                                            const uint32_t* __restrict__ map,
-                                                            const uint32_t* __restrict__ tile_off,
-                                                            uint32_t ntiles, int32_t* out, int32_t* tmp,
-                                                            unsigned long long* cursor) {
-  __shared__ uint32_t h[256];
-  __shared__ unsigned long long start[256];
+// Each tile: regroup its ids by window in shared memory, reserve the window
+// ranges with one atomic per nonempty window, write contiguous runs.
+__global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restrict__ jobs,
+                                                              const uint32_t* __restrict__ map,
+                                                              const uint32_t* __restrict__ tile_off,
+                                                              uint32_t ntiles, const int32_t* __restrict__ src,
+                                                              int32_t* __restrict__ dst, uint32_t G,
+                                                              unsigned long long* wcur) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned long long* gstart = reinterpret_cast<unsigned long long*>(smem_raw);   // G
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(gstart + G);                        // G
+  uint32_t* lbase = cnt + G;                                                       // G
+  uint32_t* stage = lbase + G;                                                     // kTile
+  __shared__ uint32_t wt[kTileThreads / 32];
+  const uint32_t lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  const uint32_t per = (G + kTileThreads - 1) / kTileThreads;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    h[threadIdx.x] = 0;
+    for (uint32_t w = threadIdx.x; w < G; w += kTileThreads) cnt[w] = 0;
     __syncthreads();
     const uint32_t j = map[t];
     const Job jb = jobs[j];
-    const bool in_tmp = (jb.info & 1u) != 0;
-    const int32_t* src = in_tmp ? tmp : out;
-    int32_t* dst = in_tmp ? out : tmp;
-    const uint32_t hibit = (jb.info >> 8) & 255u;
-    const uint32_t k = t - tile_off[j];
-    const uint32_t b0 = k * kTile;
-    const uint32_t b1 = min(b0 + kTile, jb.size);
-    for (uint32_t i = b0 + threadIdx.x; i < b1; i += SS_THREADS)
-      atomicAdd(&h[msd_digit((uint32_t)src[jb.off + i], hibit)], 1u);
+    const uint32_t b0 = (t - tile_off[j]) * kTile;
+    const uint32_t n = min(b0 + kTile, jb.size) - b0;
+    for (uint32_t i = threadIdx.x; i < n; i += kTileThreads)
+      atomicAdd(&cnt[(uint32_t)src[jb.off + b0 + i] >> kWinBits], 1u);
     __syncthreads();
-    const uint32_t c = h[threadIdx.x];
-    if (c) start[threadIdx.x] = atomicAdd(&cursor[(size_t)j * 256 + threadIdx.x], (unsigned long long)c);
-    h[threadIdx.x] = 0;
+    // exclusive scan of cnt -> lbase (each thread owns `per` consecutive windows)
+    const uint32_t w0 = threadIdx.x * per;
+    uint32_t s = 0;
+    for (uint32_t k = 0; k < per; ++k)
+      if (w0 + k < G) s += cnt[w0 + k];
+    uint32_t x = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) wt[wp] = x;
     __syncthreads();
-    for (uint32_t i = b0 + threadIdx.x; i < b1; i += SS_THREADS) {
-      const int32_t id = src[jb.off + i];
-      const uint32_t d = msd_digit((uint32_t)id, hibit);
-      const uint32_t r = atomicAdd(&h[d], 1u);
-      dst[start[d] + r] = id;
+    uint32_t run = x - s;
+    for (uint32_t k = 0; k < wp; ++k) run += wt[k];
+    __syncthreads();  // everyone has read wt before the next tile rewrites it
+    for (uint32_t k = 0; k < per; ++k) {
+      const uint32_t w = w0 + k;
+      if (w < G) {
+        const uint32_t c = cnt[w];
+        lbase[w] = run;
+        if (c) gstart[w] = atomicAdd(&wcur[(size_t)j * G + w], (unsigned long long)c);
+        run += c;
+        cnt[w] = 0;
+      }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += kTileThreads) {
+      const uint32_t id = (uint32_t)src[jb.off + b0 + i];
+      const uint32_t w = id >> kWinBits;
+      stage[lbase[w] + atomicAdd(&cnt[w], 1u)] = id;
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += kTileThreads) {
+      const uint32_t id = stage[i];
+      const uint32_t w = id >> kWinBits;
+      dst[gstart[w] + (i - lbase[w])] = (int32_t)id;
     }
     __syncthreads();
   }
 }
 
-// One CTA per (job, bucket): sort buckets that fit shared memory into out,
-// queue the others for the next round.
-__global__ void __launch_bounds__(SS_THREADS) k_msd_buckets(const Job* __restrict__ jobs, uint32_t njobs,
-                                                            const uint32_t* __restrict__ hist,
-                                                            const unsigned long long* __restrict__ base,
-                                                            int32_t* out, int32_t* tmp, Job* next,
-                                                            uint32_t* nnext, uint32_t next_cap,
-                                                            uint32_t* overflow) {
-  __shared__ uint32_t sa[kCap];
-  __shared__ uint32_t sb[kCap];
-  __shared__ uint32_t wcnt[SS_WARPS][256];
-  __shared__ uint32_t dig_excl[256];
-  __shared__ uint32_t wtot[SS_WARPS];
-  const uint64_t total = (uint64_t)njobs * 256;
+// One CTA per (job, window): sort the window's ids from src into out.
+// With G == 1 the window is the whole slice and src == out: every id is read
+// into shared memory before any is written, so sorting in place is safe.
+__global__ void __launch_bounds__(kSortThreads) k_win_sort(
+    const Job* __restrict__ jobs, uint32_t njobs, uint32_t G, uint32_t wbits,
+    const uint32_t* __restrict__ whist, const unsigned long long* __restrict__ wbase,
+    const int32_t* src, int32_t* out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t* bm = reinterpret_cast<uint32_t*>(smem_raw);   // bitmap, W/32 words
+  RadixSmem& rs = *reinterpret_cast<RadixSmem*>(smem_raw);
+  __shared__ uint32_t wtot[kSortWarps];
+  __shared__ uint32_t wpos[kSortWarps];
+  const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  const uint32_t nwords = ((1u << wbits) + 31) >> 5;
+  const uint64_t total = (uint64_t)njobs * G;
   for (uint64_t g = blockIdx.x; g < total; g += gridDim.x) {
-    const uint32_t j = (uint32_t)(g >> 8), bkt = (uint32_t)(g & 255);
-    const uint32_t size = hist[(size_t)j * 256 + bkt];
+    const uint32_t j = (uint32_t)(g / G), w = (uint32_t)(g % G);
+    uint32_t size;
+    unsigned long long off;
+    if (G == 1) {
+      size = jobs[j].size;
+      off = jobs[j].off;
+    } else {
+      size = whist[g];
+      off = wbase[g];
+    }
     if (size == 0) continue;
-    const Job jb = jobs[j];
-    const bool data_in_tmp = (jb.info & 1u) == 0;  // the scatter moved it to the other buffer
-    const uint32_t hibit = (jb.info >> 8) & 255u;
-    const uint32_t lo = hibit > 8 ? hibit - 8 : 0;
-    const unsigned long long off = base[(size_t)j * 256 + bkt];
-    if (size <= kCap) {
-      sort_slice(data_in_tmp ? tmp : out, out, off, size, lo, sa, sb, wcnt, dig_excl, wtot);
-    } else if (lo == 0) {
-      // more than kCap ids share every bit: only possible with repeated ids
-      if (threadIdx.x == 0) atomicOr(overflow, 2u);
-    } else if (threadIdx.x == 0) {
-      const uint32_t slot = atomicAdd(nnext, 1u);
-      if (slot < next_cap) {
-        Job nj;
-        nj.off = off;
-        nj.size = size;
-        nj.info = (lo << 8) | (data_in_tmp ? 1u : 0u);
-        next[slot] = nj;
-      } else {
-        atomicOr(overflow, 1u);
+    const uint32_t lo = w << wbits;
+    if (size == 1) {
+      if (tid == 0) out[off] = src[off];
+      continue;
+    }
+    if ((uint64_t)nwords > 8ull * size) {
+      // sparse window: radix sort on the low wbits (size < W/256 <= kSmallCap)
+      for (uint32_t i = tid; i < size; i += kSortThreads) rs.a[i] = (uint32_t)src[off + i] - lo;
+      __syncthreads();
+      radix_sort_smem(rs, size, wbits);
+      for (uint32_t i = tid; i < size; i += kSortThreads) out[off + i] = (int32_t)(rs.a[i] + lo);
+      __syncthreads();
+      continue;
+    }
+    // dense window: bitmap
+    for (uint32_t i = tid; i < nwords; i += kSortThreads) bm[i] = 0u;
+    __syncthreads();
+    for (uint32_t i = tid; i < size; i += kSortThreads) {
+      const uint32_t rel = (uint32_t)src[off + i] - lo;
+      atomicOr(&bm[rel >> 5], 1u << (rel & 31));
+    }
+    __syncthreads();
+    // each warp owns a contiguous block of words
+    const uint32_t per_warp = (nwords + kSortWarps - 1) / kSortWarps;
+    const uint32_t a0 = min(wp * per_warp, nwords);
+    const uint32_t a1 = min(a0 + per_warp, nwords);
+    uint32_t c = 0;
+    for (uint32_t k = a0 + lane; k < a1; k += 32) c += __popc(bm[k]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) wtot[wp] = c;
+    __syncthreads();
+    if (tid == 0) {
+      uint32_t r = 0;
+      for (uint32_t k = 0; k < kSortWarps; ++k) {
+        wpos[k] = r;
+        r += wtot[k];
       }
     }
+    __syncthreads();
+    uint32_t pos = wpos[wp];
+    for (uint32_t k0 = a0; k0 < a1; k0 += 32) {
+      const uint32_t k = k0 + lane;
+      uint32_t word = (k < a1) ? bm[k] : 0u;
+      const uint32_t pc = __popc(word);
+      uint32_t x = pc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+      }
+      const uint32_t tot = __shfl_sync(0xffffffffu, x, 31);
+      unsigned long long o = off + pos + (x - pc);
+      const uint32_t base_id = lo + (k << 5);
+      while (word) {
+        const int b = __ffs(word) - 1;
+        word &= word - 1;
+        out[o++] = (int32_t)(base_id + (uint32_t)b);
+      }
+      pos += tot;
+    }
+    __syncthreads();
   }
 }
 
@@ -315,101 +402,104 @@ __global__ void __launch_bounds__(SS_THREADS) k_msd_buckets(const Job* __restric
 
 qcp_status ws_reserve_sort(qcp_index* ix, Workspace* ws, size_t jobs, size_t tiles);
 
-// Workspace layout used here: ws->jobs[0] small jobs, ws->jobs[1] big jobs
-// (both `jobs_cap` entries of 16 bytes); the MSD tables live in ix->pool.
 qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t s) {
   ws->sort_small_jobs = ws->sort_msd_jobs = 0;
   if (q == 0) return QCP_OK;
   uint32_t idbits = 1;
   while (idbits < 31 && (1ull << idbits) < ix->n) ++idbits;
+  const uint32_t wbits = idbits < kWinBits ? idbits : kWinBits;
+  const uint32_t G = 1u << (idbits - wbits);
   const uint32_t sms = (uint32_t)num_sms();
-  // job lists: one entry per query, and at most total/kCap oversized buckets
-  const size_t njobs_max = (size_t)q + (size_t)(*ws->h_total / kCap) + 256;
-  QCP_TRY(ws_reserve_sort(ix, ws, njobs_max, 0));
+
+  const size_t radix_bytes = sizeof(RadixSmem);
+  const size_t bitmap_bytes = ((size_t)1 << kWinBits) / 8;
+  const size_t win_bytes = radix_bytes > bitmap_bytes ? radix_bytes : bitmap_bytes;
+  const size_t scatter_bytes = (size_t)G * 16 + kTile * 4;
+  static thread_local int attrs_device = -1;  // attributes are per device
+  if (attrs_device != ix->device) {
+    QCP_CUDA(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)radix_bytes));
+    QCP_CUDA(cudaFuncSetAttribute(k_win_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)win_bytes));
+    QCP_CUDA(cudaFuncSetAttribute(k_win_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)((size_t)kMaxWindows * 16 + kTile * 4)));
+    attrs_device = ix->device;
+  }
+
+  QCP_TRY(ws_reserve_sort(ix, ws, (size_t)q + 256, 0));
   uint32_t* ctr = ws->ctr;
-  QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t) * 3, s));
+  QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t) * 2, s));
   Job* small = reinterpret_cast<Job*>(ws->jobs[0]);
   Job* big = reinterpret_cast<Job*>(ws->jobs[1]);
-  k_classify<<<(q + 255) / 256, 256, 0, s>>>((const unsigned long long*)ws->offsets, q, idbits, small,
+  k_classify<<<(q + 255) / 256, 256, 0, s>>>((const unsigned long long*)ws->offsets, q, small,
                                              ctr + kCtrJobs0, big, ctr + kCtrJobs1);
   note_launch();
   QCP_CUDA(cudaMemcpyAsync(ws->h_ctr, ctr, sizeof(uint32_t) * kCtrCount, cudaMemcpyDeviceToHost, s));
   QCP_CUDA(cudaStreamSynchronize(s));
   const uint32_t nsmall = ws->h_ctr[kCtrJobs0];
-  uint32_t nbig = ws->h_ctr[kCtrJobs1];
+  const uint32_t nbig = ws->h_ctr[kCtrJobs1];
   ws->sort_small_jobs = nsmall;
-  ws->sort_msd_jobs = 0;
+  ws->sort_msd_jobs = nbig;
   if (nsmall) {
-    k_sort_small<<<min(nsmall, sms * 16), SS_THREADS, 0, s>>>(small, nsmall, ws->out_ids, ws->tmp_ids);
+    k_sort_small<<<min(nsmall, sms * 4), kSortThreads, radix_bytes, s>>>(small, nsmall, ws->out_ids, idbits);
     note_launch();
+    QCP_TRY(check_launch("k_sort_small"));
   }
-  QCP_TRY(check_launch("k_sort_small"));
-  // MSD rounds over the big jobs; the job list of a round lives in `cur`.
-  Job* cur = big;
+  if (nbig == 0) return QCP_OK;
+
+  if (G == 1) {
+    k_win_sort<<<min(nbig, sms * 4), kSortThreads, win_bytes, s>>>(big, nbig, 1, wbits, nullptr, nullptr,
+                                                                   ws->out_ids, ws->out_ids);
+    note_launch();
+    return check_launch("k_win_sort");
+  }
+
+  // window partition tables: whist (u32), wbase, wcur (u64) per (job, window);
+  // tiles and tile offsets per job
+  const size_t nw = (size_t)nbig * G;
+  const size_t hist_bytes = (nw * 4 + 15) & ~(size_t)15;
+  const size_t bytes = hist_bytes + nw * 16 + (size_t)nbig * 8 + 64;
   void* tables = nullptr;
-  size_t tables_bytes = 0;
+  QCP_TRY(ix->pool.get(bytes, &tables));
+  uint32_t* whist = reinterpret_cast<uint32_t*>(tables);
+  unsigned long long* wbase = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(tables) + hist_bytes);
+  unsigned long long* wcur = wbase + nw;
+  uint32_t* tiles = reinterpret_cast<uint32_t*>(wcur + nw);
+  uint32_t* tile_off = tiles + nbig;
   qcp_status st = QCP_OK;
-  for (int round = 0; round < 4 && nbig > 0 && st == QCP_OK; ++round) {
-    ws->sort_msd_jobs += nbig;
-    const size_t need = (size_t)nbig * 256 * (4 + 8 + 8) + (size_t)nbig * 8 + 16;
-    if (need > tables_bytes) {
-      if (tables) ix->pool.put(tables_bytes, tables);
-      tables = nullptr;
-      tables_bytes = need;
-      st = ix->pool.get(tables_bytes, &tables);
-      if (st != QCP_OK) {
-        tables_bytes = 0;
-        break;
-      }
-    }
-    uint32_t* hist = reinterpret_cast<uint32_t*>(tables);
-    unsigned long long* base = reinterpret_cast<unsigned long long*>(hist + (size_t)nbig * 256);
-    unsigned long long* cursor = base + (size_t)nbig * 256;
-    uint32_t* tiles = reinterpret_cast<uint32_t*>(cursor + (size_t)nbig * 256);
-    uint32_t* tile_off = tiles + nbig;
-    // tiles per job -> offsets -> tile map
-    k_tiles_per_job<<<(nbig + 255) / 256, 256, 0, s>>>(cur, nbig, tiles);
+  do {
+    k_tiles_per_job<<<(nbig + 255) / 256, 256, 0, s>>>(big, nbig, tiles);
     note_launch();
     st = exclusive_scan<uint32_t>(tiles, tile_off, nbig, ctr + kCtrWork2, ix->pool, s);
     if (st != QCP_OK) break;
-    QCP_CUDA(cudaMemcpyAsync(ws->h_ctr + kCtrWork2, ctr + kCtrWork2, sizeof(uint32_t),
-                             cudaMemcpyDeviceToHost, s));
-    QCP_CUDA(cudaStreamSynchronize(s));
+    if (cudaMemcpyAsync(ws->h_ctr + kCtrWork2, ctr + kCtrWork2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      st = cuda_status(cudaGetLastError(), "segmented sort tiles");
+      break;
+    }
     const uint32_t ntiles = ws->h_ctr[kCtrWork2];
     st = ws_reserve_sort(ix, ws, 0, ntiles);
     if (st != QCP_OK) break;
-    uint32_t* map = reinterpret_cast<uint32_t*>(ws->seg_hist);
+    uint32_t* map = ws->seg_hist;
     k_tile_map<<<min(nbig, sms * 8), 256, 0, s>>>(tiles, tile_off, nbig, map);
-    QCP_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 256 * (size_t)nbig, s));
-    k_msd_hist<<<min(ntiles, sms * 16), SS_THREADS, 0, s>>>(cur, map, tile_off, ntiles, ws->out_ids,
-                                                            ws->tmp_ids, hist);
-    k_msd_scan<<<min(nbig, sms * 16), SS_THREADS, 0, s>>>(cur, nbig, hist, base, cursor);
-    k_msd_scatter<<<min(ntiles, sms * 16), SS_THREADS, 0, s>>>(cur, map, tile_off, ntiles, ws->out_ids,
-                                                               ws->tmp_ids, cursor);
-    note_launch(4);
-    // next round's jobs go to the other list
-    Job* next = (cur == big) ? small : big;
-    QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t), s));
-    QCP_CUDA(cudaMemsetAsync(ctr + kCtrOverflow, 0, sizeof(uint32_t), s));
-    const uint64_t grid = (uint64_t)nbig * 256;
-    k_msd_buckets<<<(uint32_t)(grid < (uint64_t)sms * 16 ? grid : (uint64_t)sms * 16), SS_THREADS, 0, s>>>(
-        cur, nbig, hist, base, ws->out_ids, ws->tmp_ids, next, ctr + kCtrJobs0,
-        (uint32_t)ws->jobs_cap, ctr + kCtrOverflow);
-    note_launch();
-    st = check_launch("segmented_sort MSD round");
-    if (st != QCP_OK) break;
-    QCP_CUDA(cudaMemcpyAsync(ws->h_ctr, ctr, sizeof(uint32_t) * kCtrCount, cudaMemcpyDeviceToHost, s));
-    QCP_CUDA(cudaStreamSynchronize(s));
-    if (ws->h_ctr[kCtrOverflow]) {
-      set_error((ws->h_ctr[kCtrOverflow] & 2u) ? "segmented sort: repeated ids in one result"
-                                               : "segmented sort: job list overflow");
-      st = QCP_ERR_CUDA;
+    if (cudaMemsetAsync(whist, 0, sizeof(uint32_t) * nw, s) != cudaSuccess) {
+      st = cuda_status(cudaGetLastError(), "memset");
       break;
     }
-    nbig = ws->h_ctr[kCtrJobs0];
-    cur = next;
-  }
-  if (tables) ix->pool.put(tables_bytes, tables);
+    k_win_hist<<<min(ntiles, sms * 16), kTileThreads, sizeof(uint32_t) * G, s>>>(big, map, tile_off, ntiles,
+                                                                                 ws->out_ids, G, whist);
+    k_win_scan<<<min(nbig, sms * 16), kTileThreads, 0, s>>>(big, nbig, G, whist, wbase, wcur);
+    k_win_scatter<<<min(ntiles, sms * 8), kTileThreads, scatter_bytes, s>>>(big, map, tile_off, ntiles,
+                                                                            ws->out_ids, ws->tmp_ids, G, wcur);
+    const uint64_t regions = (uint64_t)nbig * G;
+    const uint32_t grid = (uint32_t)(regions < (uint64_t)sms * 4 ? regions : (uint64_t)sms * 4);
+    k_win_sort<<<grid, kSortThreads, win_bytes, s>>>(big, nbig, G, wbits, whist, wbase, ws->tmp_ids,
+                                                     ws->out_ids);
+    note_launch(5);
+    st = check_launch("segmented sort windows");
+    // the tables go back to the pool below: make sure the kernels are done
+    if (st == QCP_OK && cudaStreamSynchronize(s) != cudaSuccess) st = cuda_status(cudaGetLastError(), "sort");
+  } while (false);
+  ix->pool.put(bytes, tables);
   return st;
 }
 

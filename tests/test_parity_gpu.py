@@ -25,6 +25,7 @@ def test_golden_cases_exact(qcp, oracle, cases, name, algo):
     with qcp.Index.build(objs) as ix:
         res = ix.search(boxes, algo=algo)
         assert_same_hits(res.offsets, res.ids, want_offs, want_ids, boxes)
+        assert res.total_hits == int(ref_counts.sum())
         assert np.array_equal(ix.counts(boxes, algo=algo), ref_counts)
 
 
@@ -86,7 +87,7 @@ class _DeviceArray:
     """A non-owning view of library-owned device memory for torch.as_tensor."""
 
     def __init__(self, ptr: int, n: int, typestr: str):
-        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (int(ptr), True),
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (int(ptr), False),
                                          "version": 3}
 
 
@@ -180,3 +181,18 @@ def test_repeated_calls_reuse_buffers(qcp, oracle, cases):
             assert_same_hits(res.offsets, res.ids, o, i)
         res = ix.search(boxes)
         assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
+
+
+@pytest.mark.parametrize("n", [300_000, 2_000_000])
+def test_large_result_slices(qcp, oracle, workloads, n):
+    """Slices far above the shared-memory sort size: one id window (n <= 2^19)
+    and many windows (n > 2^19), dense and sparse windows."""
+    pts = workloads.gaussian_mixture_points(n, 3, seed=99)
+    boxes = workloads.data_centred_cubes(pts, 40, 1e-5, 3e-2, seed=98)
+    boxes = np.concatenate([boxes, np.array([[-1, -1, -1, 2, 2, 2]], np.float32)])  # everything
+    want_offs, want_ids = oracle.ids(pts, 3, False, boxes, threads=16)
+    assert np.diff(want_offs).max() > 100_000
+    with qcp.Index.build(pts) as ix:
+        for algo in ["batched", "plain"]:
+            res = ix.search(boxes, algo=algo)
+            assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
