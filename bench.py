@@ -148,7 +148,9 @@ def run_ours(args, rank, world, local):
     else:
         w = W.config2(q=q_per_rank * world)
         boxes_all = w.boxes
-    boxes = np.ascontiguousarray(boxes_all[rank * q_per_rank:(rank + 1) * q_per_rank])
+    import qcp_b200.sharding as S
+    a, b = S.query_shard(len(boxes_all), rank, world)
+    boxes = np.ascontiguousarray(boxes_all[a:b])
     Q = boxes.shape[0]
 
     d_objs = torch.from_numpy(w.objs).to(dev)

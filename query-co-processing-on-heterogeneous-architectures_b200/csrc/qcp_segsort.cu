@@ -16,12 +16,13 @@
 //                               bases -> each tile regrouped by window in
 //                               shared memory and written as contiguous runs
 //                               into the scratch buffer);
-//                            2. one CTA per (slice, window): a window of
-//                               W = 2^kWinBits possible ids is a 64 KiB bitmap
-//                               in shared memory; dense windows set a bit per
-//                               id and compact the bitmap in order, sparse
-//                               windows (fewer than one id per 8 bitmap
-//                               words) use the radix sort instead.
+//                            2. persistent CTAs over the (slice, window)
+//                               regions: a window of W = 2^kWinBits possible
+//                               ids is a 64 KiB bitmap plus a 2 KiB summary
+//                               (one bit per nonzero bitmap word) in shared
+//                               memory; ids set their bits, then each thread
+//                               compacts the words under one summary word in
+//                               order, so the cost follows the ids, not W.
 //                            With idbits <= kWinBits there is one window and
 //                            step 1 is skipped (the slice is sorted in place).
 #include "qcp_internal.cuh"
@@ -38,6 +39,8 @@ constexpr uint32_t kWinBits = 19;      // 2^19 ids per window -> 64 KiB bitmap
 constexpr uint32_t kTile = 4096;       // ids per partition tile
 constexpr uint32_t kTileThreads = 256;
 constexpr uint32_t kMaxWindows = 1u << (31 - kWinBits);
+constexpr uint32_t kBmWords = (1u << kWinBits) / 32;   // 16384 bitmap words
+constexpr uint32_t kSumWords = kBmWords / 32;           // 512 summary words
 
 struct Job {
   unsigned long long off;
@@ -251,6 +254,7 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
   uint32_t* cnt = reinterpret_cast<uint32_t*>(gstart + G);                        // G
   uint32_t* lbase = cnt + G;                                                       // G
   uint32_t* stage = lbase + G;                                                     // kTile
+  uint32_t* raw = stage + kTile;                                                   // kTile
   __shared__ uint32_t wt[kTileThreads / 32];
   const uint32_t lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   const uint32_t per = (G + kTileThreads - 1) / kTileThreads;
@@ -261,8 +265,11 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
     const Job jb = jobs[j];
     const uint32_t b0 = (t - tile_off[j]) * kTile;
     const uint32_t n = min(b0 + kTile, jb.size) - b0;
-    for (uint32_t i = threadIdx.x; i < n; i += kTileThreads)
-      atomicAdd(&cnt[(uint32_t)src[jb.off + b0 + i] >> kWinBits], 1u);
+    for (uint32_t i = threadIdx.x; i < n; i += kTileThreads) {
+      const uint32_t id = (uint32_t)src[jb.off + b0 + i];
+      raw[i] = id;
+      atomicAdd(&cnt[id >> kWinBits], 1u);
+    }
     __syncthreads();
     // exclusive scan of cnt -> lbase (each thread owns `per` consecutive windows)
     const uint32_t w0 = threadIdx.x * per;
@@ -292,7 +299,7 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < n; i += kTileThreads) {
-      const uint32_t id = (uint32_t)src[jb.off + b0 + i];
+      const uint32_t id = raw[i];
       const uint32_t w = id >> kWinBits;
       stage[lbase[w] + atomicAdd(&cnt[w], 1u)] = id;
     }
@@ -306,20 +313,27 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
   }
 }
 
-// One CTA per (job, window): sort the window's ids from src into out.
-// With G == 1 the window is the whole slice and src == out: every id is read
-// into shared memory before any is written, so sorting in place is safe.
+// Persistent CTAs over the (job, window) regions: sort each window's ids
+// from src into out with a two-level bitmap in shared memory.  Insertion sets
+// the id's bit and the bit of its word in a summary bitmap; compaction gives
+// every thread one summary word (32 bitmap words), counts the ids under it,
+// takes its output position from a block scan and writes its ids in order,
+// clearing the words it read.  Work per region is proportional to its ids,
+// not to the window width.  With G == 1 the window is the whole slice and
+// src == out: all ids are inserted before any is written.
 __global__ void __launch_bounds__(kSortThreads) k_win_sort(
     const Job* __restrict__ jobs, uint32_t njobs, uint32_t G, uint32_t wbits,
     const uint32_t* __restrict__ whist, const unsigned long long* __restrict__ wbase,
     const int32_t* src, int32_t* out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint32_t* bm = reinterpret_cast<uint32_t*>(smem_raw);   // bitmap, W/32 words
-  RadixSmem& rs = *reinterpret_cast<RadixSmem*>(smem_raw);
+  uint32_t* bm = reinterpret_cast<uint32_t*>(smem_raw);  // kBmWords
+  uint32_t* sm = bm + kBmWords;                          // kSumWords
   __shared__ uint32_t wtot[kSortWarps];
-  __shared__ uint32_t wpos[kSortWarps];
   const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   const uint32_t nwords = ((1u << wbits) + 31) >> 5;
+  const uint32_t nsum = (nwords + 31) >> 5;  // <= kSortThreads
+  for (uint32_t i = tid; i < kBmWords + kSumWords; i += kSortThreads) bm[i] = 0u;
+  __syncthreads();
   const uint64_t total = (uint64_t)njobs * G;
   for (uint64_t g = blockIdx.x; g < total; g += gridDim.x) {
     const uint32_t j = (uint32_t)(g / G), w = (uint32_t)(g % G);
@@ -338,62 +352,39 @@ __global__ void __launch_bounds__(kSortThreads) k_win_sort(
       if (tid == 0) out[off] = src[off];
       continue;
     }
-    if ((uint64_t)nwords > 8ull * size) {
-      // sparse window: radix sort on the low wbits (size < W/256 <= kSmallCap)
-      for (uint32_t i = tid; i < size; i += kSortThreads) rs.a[i] = (uint32_t)src[off + i] - lo;
-      __syncthreads();
-      radix_sort_smem(rs, size, wbits);
-      for (uint32_t i = tid; i < size; i += kSortThreads) out[off + i] = (int32_t)(rs.a[i] + lo);
-      __syncthreads();
-      continue;
-    }
-    // dense window: bitmap
-    for (uint32_t i = tid; i < nwords; i += kSortThreads) bm[i] = 0u;
-    __syncthreads();
     for (uint32_t i = tid; i < size; i += kSortThreads) {
       const uint32_t rel = (uint32_t)src[off + i] - lo;
-      atomicOr(&bm[rel >> 5], 1u << (rel & 31));
+      const uint32_t word = rel >> 5;
+      atomicOr(&bm[word], 1u << (rel & 31));
+      atomicOr(&sm[word >> 5], 1u << (word & 31));
     }
     __syncthreads();
-    // each warp owns a contiguous block of words
-    const uint32_t per_warp = (nwords + kSortWarps - 1) / kSortWarps;
-    const uint32_t a0 = min(wp * per_warp, nwords);
-    const uint32_t a1 = min(a0 + per_warp, nwords);
+    const uint32_t s = (tid < nsum) ? sm[tid] : 0u;
     uint32_t c = 0;
-    for (uint32_t k = a0 + lane; k < a1; k += 32) c += __popc(bm[k]);
+    for (uint32_t m = s; m; m &= m - 1) c += __popc(bm[tid * 32 + __ffs(m) - 1]);
+    uint32_t x = c;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if (lane == 0) wtot[wp] = c;
-    __syncthreads();
-    if (tid == 0) {
-      uint32_t r = 0;
-      for (uint32_t k = 0; k < kSortWarps; ++k) {
-        wpos[k] = r;
-        r += wtot[k];
-      }
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (uint32_t)o) x += y;
     }
+    if (lane == 31) wtot[wp] = x;
     __syncthreads();
-    uint32_t pos = wpos[wp];
-    for (uint32_t k0 = a0; k0 < a1; k0 += 32) {
-      const uint32_t k = k0 + lane;
-      uint32_t word = (k < a1) ? bm[k] : 0u;
-      const uint32_t pc = __popc(word);
-      uint32_t x = pc;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= (uint32_t)o) x += y;
-      }
-      const uint32_t tot = __shfl_sync(0xffffffffu, x, 31);
-      unsigned long long o = off + pos + (x - pc);
-      const uint32_t base_id = lo + (k << 5);
-      while (word) {
-        const int b = __ffs(word) - 1;
-        word &= word - 1;
+    uint32_t before = x - c;
+    for (uint32_t k = 0; k < wp; ++k) before += wtot[k];
+    unsigned long long o = off + before;
+    for (uint32_t m = s; m; m &= m - 1) {
+      const uint32_t wd = tid * 32 + __ffs(m) - 1;
+      uint32_t bits = bm[wd];
+      bm[wd] = 0u;
+      const uint32_t base_id = lo + (wd << 5);
+      while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1;
         out[o++] = (int32_t)(base_id + (uint32_t)b);
       }
-      pos += tot;
     }
+    if (tid < nsum) sm[tid] = 0u;
     __syncthreads();
   }
 }
@@ -412,15 +403,14 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   const uint32_t sms = (uint32_t)num_sms();
 
   const size_t radix_bytes = sizeof(RadixSmem);
-  const size_t bitmap_bytes = ((size_t)1 << kWinBits) / 8;
-  const size_t win_bytes = radix_bytes > bitmap_bytes ? radix_bytes : bitmap_bytes;
-  const size_t scatter_bytes = (size_t)G * 16 + kTile * 4;
+  const size_t win_bytes = sizeof(uint32_t) * (kBmWords + kSumWords);
+  const size_t scatter_bytes = (size_t)G * 16 + kTile * 8;
   static thread_local int attrs_device = -1;  // attributes are per device
   if (attrs_device != ix->device) {
     QCP_CUDA(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)radix_bytes));
     QCP_CUDA(cudaFuncSetAttribute(k_win_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)win_bytes));
     QCP_CUDA(cudaFuncSetAttribute(k_win_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)((size_t)kMaxWindows * 16 + kTile * 4)));
+                                  (int)((size_t)kMaxWindows * 16 + kTile * 8)));
     attrs_device = ix->device;
   }
 
@@ -446,7 +436,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   if (nbig == 0) return QCP_OK;
 
   if (G == 1) {
-    k_win_sort<<<min(nbig, sms * 4), kSortThreads, win_bytes, s>>>(big, nbig, 1, wbits, nullptr, nullptr,
+    k_win_sort<<<min(nbig, sms * 3), kSortThreads, win_bytes, s>>>(big, nbig, 1, wbits, nullptr, nullptr,
                                                                    ws->out_ids, ws->out_ids);
     note_launch();
     return check_launch("k_win_sort");
@@ -491,7 +481,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
     k_win_scatter<<<min(ntiles, sms * 8), kTileThreads, scatter_bytes, s>>>(big, map, tile_off, ntiles,
                                                                             ws->out_ids, ws->tmp_ids, G, wcur);
     const uint64_t regions = (uint64_t)nbig * G;
-    const uint32_t grid = (uint32_t)(regions < (uint64_t)sms * 4 ? regions : (uint64_t)sms * 4);
+    const uint32_t grid = (uint32_t)(regions < (uint64_t)sms * 3 ? regions : (uint64_t)sms * 3);
     k_win_sort<<<grid, kSortThreads, win_bytes, s>>>(big, nbig, G, wbits, whist, wbase, ws->tmp_ids,
                                                      ws->out_ids);
     note_launch(5);
