@@ -188,7 +188,8 @@ def run_ours(args, rank, world, local):
     barrier()
     torch.cuda.synchronize()
     qcp.launch_count(reset=True)
-    phase = {"expand": 0.0, "count": 0.0, "scan": 0.0, "write": 0.0, "sort": 0.0, "total": 0.0}
+    phase = {"expand": 0.0, "count": 0.0, "scan": 0.0, "write": 0.0, "sort": 0.0, "total": 0.0,
+             "sort_small": 0.0, "sort_partition": 0.0, "sort_windows": 0.0}
     step_ms = []
     stats = None
     ev0 = torch.cuda.Event(enable_timing=True)

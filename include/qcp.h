@@ -126,6 +126,8 @@ typedef struct qcp_query_stats {
   uint32_t sort_msd_jobs;      /* slices split by MSD rounds (all rounds) */
   /* device milliseconds per phase (only with QCP_QUERY_TIMING) */
   float ms_expand, ms_count, ms_scan, ms_write, ms_sort, ms_total;
+  /* parts of ms_sort: small slices, window partition, window sort */
+  float ms_sort_small, ms_sort_partition, ms_sort_windows;
 } qcp_query_stats;
 
 qcp_status qcp_query_stats_last(qcp_query_stats* out);

@@ -69,7 +69,9 @@ class QueryStats(ctypes.Structure):
                 ("sort_small_jobs", ctypes.c_uint32), ("sort_msd_jobs", ctypes.c_uint32),
                 ("ms_expand", ctypes.c_float), ("ms_count", ctypes.c_float),
                 ("ms_scan", ctypes.c_float), ("ms_write", ctypes.c_float),
-                ("ms_sort", ctypes.c_float), ("ms_total", ctypes.c_float)]
+                ("ms_sort", ctypes.c_float), ("ms_total", ctypes.c_float),
+                ("ms_sort_small", ctypes.c_float), ("ms_sort_partition", ctypes.c_float),
+                ("ms_sort_windows", ctypes.c_float)]
 
 
 class Result(ctypes.Structure):

@@ -239,7 +239,7 @@ qcp_status ws_reserve_queries(qcp_index* ix, Workspace* ws, uint32_t q) {
     QCP_CUDA(cudaMalloc(&ws->d_stats, sizeof(unsigned long long) * kStatCount));
     QCP_CUDA(cudaMemset(ws->d_stats, 0, sizeof(unsigned long long) * kStatCount));
     QCP_CUDA(cudaHostAlloc(&ws->h_stats, sizeof(unsigned long long) * kStatCount, cudaHostAllocDefault));
-    for (int i = 0; i < 8; ++i) QCP_CUDA(cudaEventCreate(&ws->ev[i]));
+    for (int i = 0; i < kEvCountSlots; ++i) QCP_CUDA(cudaEventCreate(&ws->ev[i]));
   }
   // the root frontier holds one item per query
   if (!ws->items[0] || ws->items_cap < q) {
@@ -308,7 +308,7 @@ static void ws_destroy(Workspace* ws, qcp_index* ix) {
   if (ws->h_total) cudaFreeHost(ws->h_total);
   cudaFree(ws->d_stats);
   if (ws->h_stats) cudaFreeHost(ws->h_stats);
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < kEvCountSlots; ++i)
     if (ws->ev[i]) cudaEventDestroy(ws->ev[i]);
   delete ws;
 }
@@ -593,6 +593,15 @@ static qcp_status run_query(qcp_index* ix, const float* boxes, uint32_t q, const
         t_stats.ms_write = ms(kEvScan, kEvWrite);
         t_stats.ms_sort = ms(kEvWrite, kEvSort);
         t_stats.ms_total = ms(kEvStart, kEvSort);
+        if (!o.unsorted) {
+          t_stats.ms_sort_small = ms(kEvWrite, kEvSortSmall);
+          if (ws->sort_part_marked) {
+            t_stats.ms_sort_partition = ms(kEvSortSmall, kEvSortPart);
+            t_stats.ms_sort_windows = ms(kEvSortPart, kEvSort);
+          } else {
+            t_stats.ms_sort_windows = ms(kEvSortSmall, kEvSort);
+          }
+        }
       } else {
         t_stats.ms_total = ms(kEvStart, kEvScan);
       }

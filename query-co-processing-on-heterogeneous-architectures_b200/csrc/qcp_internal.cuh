@@ -69,6 +69,12 @@ struct DevArray {
   size_t cap = 0;  // elements
 };
 
+// Phase events of Workspace::ev.
+enum EvSlot : int {
+  kEvStart = 0, kEvExpand = 1, kEvCount = 2, kEvScan = 3, kEvWrite = 4, kEvSort = 5,
+  kEvSortSmall = 6, kEvSortPart = 7, kEvCountSlots = 8
+};
+
 // Scratch for one query call.  Reused across calls through the index's
 // workspace list (one workspace per concurrently running call).
 struct Workspace {
@@ -97,8 +103,9 @@ struct Workspace {
   // work counters (kStat* slots) and phase events of the current call
   unsigned long long* d_stats = nullptr;
   unsigned long long* h_stats = nullptr;
-  cudaEvent_t ev[8] = {};
+  cudaEvent_t ev[kEvCountSlots] = {};
   bool timing = false;
+  bool sort_part_marked = false;
   uint32_t sort_small_jobs = 0, sort_msd_jobs = 0;
 };
 
@@ -111,8 +118,6 @@ enum StatSlot : uint32_t {
   kStatCount = 24
 };
 
-// Phase events of Workspace::ev.
-enum EvSlot : int { kEvStart = 0, kEvExpand = 1, kEvCount = 2, kEvScan = 3, kEvWrite = 4, kEvSort = 5 };
 
 inline void mark(Workspace* ws, int slot, cudaStream_t s) {
   if (ws->timing) cudaEventRecord(ws->ev[slot], s);

@@ -7,9 +7,11 @@
 // `idbits` = ceil(log2 n) bits carry order, and a slice can be sorted by
 // setting one bit per id in a bitmap and reading the bitmap back in order.
 //
-//   slice <= kSmallCap ids   one 512-thread CTA sorts it in shared memory
-//                            (stable LSD radix, 8-bit digits, warp-match
-//                            ranks).
+//   slice <= kSmallCap ids   one 512-thread CTA bucket-sorts it in shared
+//                            memory: 2048 buckets by the top bits of the id,
+//                            atomic counts give every id a slot, a block scan
+//                            gives bucket bases, each bucket (a few ids) is
+//                            insertion-sorted, the order leaves coalesced.
 //   larger slices            1. window partition: ids are bucketed by
 //                               id >> kWinBits into G = 2^(idbits-kWinBits)
 //                               windows (tile histograms -> per-slice window
@@ -17,12 +19,11 @@
 //                               shared memory and written as contiguous runs
 //                               into the scratch buffer);
 //                            2. persistent CTAs over the (slice, window)
-//                               regions: a window of W = 2^kWinBits possible
-//                               ids is a 64 KiB bitmap plus a 2 KiB summary
-//                               (one bit per nonzero bitmap word) in shared
-//                               memory; ids set their bits, then each thread
-//                               compacts the words under one summary word in
-//                               order, so the cost follows the ids, not W.
+//                               regions: regions of <= kSmallCap ids are
+//                               bucket-sorted as above; denser ones set one
+//                               bit per id in a 64 KiB bitmap (plus a summary
+//                               bit per nonzero word) and compact it in
+//                               order.
 //                            With idbits <= kWinBits there is one window and
 //                            step 1 is skipped (the slice is sorted in place).
 #include "qcp_internal.cuh"
@@ -34,13 +35,14 @@ namespace {
 constexpr uint32_t kSmallCap = 8192;   // ids sorted by one CTA
 constexpr uint32_t kSortThreads = 512;
 constexpr uint32_t kSortWarps = kSortThreads / 32;
-constexpr uint32_t kRounds = kSmallCap / kSortWarps / 32;  // 16 ids per lane
 constexpr uint32_t kWinBits = 19;      // 2^19 ids per window -> 64 KiB bitmap
 constexpr uint32_t kTile = 4096;       // ids per partition tile
 constexpr uint32_t kTileThreads = 256;
 constexpr uint32_t kMaxWindows = 1u << (31 - kWinBits);
 constexpr uint32_t kBmWords = (1u << kWinBits) / 32;   // 16384 bitmap words
 constexpr uint32_t kSumWords = kBmWords / 32;           // 512 summary words
+constexpr uint32_t kBucketBits = 11;
+constexpr uint32_t kBuckets = 1u << kBucketBits;       // buckets of the region sort
 
 struct Job {
   unsigned long long off;
@@ -48,92 +50,86 @@ struct Job {
   uint32_t pad;
 };
 
-__device__ __forceinline__ uint32_t lanemask_lt_() {
-  uint32_t m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
-
-// Shared memory of the radix sort (placed at the start of dynamic smem).
-struct RadixSmem {
-  uint32_t a[kSmallCap];
-  uint32_t b[kSmallCap];
-  uint32_t wcnt[kSortWarps][256];
-  uint32_t dig_excl[256];
+// Shared memory of the bucket sort.
+struct BucketSmem {
+  uint32_t cnt[kBuckets];   // ids per bucket, then (after the scan) bucket ends
+  uint32_t base[kBuckets];  // first slot of each bucket
+  uint32_t stage[kSmallCap];
   uint32_t wtot[kSortWarps];
 };
 
-// Stable LSD sort of s.a[0..n) (n <= kSmallCap) on bits [0, hibit); the
-// result ends in s.a.  Needs blockDim.x == kSortThreads.
-__device__ void radix_sort_smem(RadixSmem& s, uint32_t n, uint32_t hibit) {
-  const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const uint32_t passes = (hibit + 7) / 8;
-  uint32_t* a = s.a;
-  uint32_t* b = s.b;
-  for (uint32_t p = 0; p < passes; ++p) {
-    const uint32_t shift = 8 * p;
-    for (uint32_t i = tid; i < kSortWarps * 256; i += kSortThreads) (&s.wcnt[0][0])[i] = 0;
-    __syncthreads();
-    uint32_t rank[kRounds];
-    uint32_t key[kRounds];
+// Sorts `size` (<= kSmallCap) distinct ids from src[off..) into out[off..)
+// (src may equal out: every id is read before any is written).  The ids lie
+// in [lo, lo + 2^wbits).  Bucket b holds ids whose offset from lo has b as
+// its top log2(kBuckets) bits; counting gives every id a slot in its bucket,
+// a block scan turns counts into bucket bases, each thread then
+// insertion-sorts the few ids of its buckets and the block copies the
+// staged order out with coalesced stores.  cnt[] must be zero on entry and
+// is zero again on exit.  Needs blockDim.x == kSortThreads.
+__device__ void bucket_sort_region(const int32_t* src, int32_t* out, unsigned long long off, uint32_t size,
+                                   uint32_t lo, uint32_t wbits, BucketSmem& s) {
+  const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  const uint32_t bshift = wbits > kBucketBits ? wbits - kBucketBits : 0;
+  constexpr uint32_t kPer = kSmallCap / kSortThreads;  // 16 ids per thread at most
+  uint32_t v[kPer];
+  uint32_t slot[kPer];
 #pragma unroll
-    for (uint32_t r = 0; r < kRounds; ++r) {
-      const uint32_t li = (w * kRounds + r) * 32 + lane;
-      const bool valid = li < n;
-      key[r] = valid ? a[li] : 0u;
-      rank[r] = 0;
-      const uint32_t active = __ballot_sync(0xffffffffu, valid);
-      if (valid) {
-        const uint32_t d = (key[r] >> shift) & 255u;
-        const uint32_t peers = __match_any_sync(active, d);
-        const uint32_t prev = s.wcnt[w][d];
-        rank[r] = prev + __popc(peers & lanemask_lt_());
-        __syncwarp(active);
-        if (lane == (uint32_t)(__ffs(peers) - 1)) s.wcnt[w][d] = prev + __popc(peers);
-        __syncwarp(active);
-      }
-    }
-    __syncthreads();
-    // digit d = tid (threads 0..255): exclusive across warps, then digits
-    uint32_t run = 0;
-    if (tid < 256) {
-      for (uint32_t k = 0; k < kSortWarps; ++k) {
-        const uint32_t c = s.wcnt[k][tid];
-        s.wcnt[k][tid] = run;
-        run += c;
-      }
-    }
-    uint32_t x = run;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= (uint32_t)o) x += y;
-    }
-    if (lane == 31 && w < 8) s.wtot[w] = x;
-    __syncthreads();
-    if (tid < 256) {
-      uint32_t before = 0;
-      for (uint32_t k = 0; k < w; ++k) before += s.wtot[k];
-      s.dig_excl[tid] = before + x - run;
-    }
-    __syncthreads();
-#pragma unroll
-    for (uint32_t r = 0; r < kRounds; ++r) {
-      const uint32_t li = (w * kRounds + r) * 32 + lane;
-      if (li < n) {
-        const uint32_t d = (key[r] >> shift) & 255u;
-        b[s.dig_excl[d] + s.wcnt[w][d] + rank[r]] = key[r];
-      }
-    }
-    __syncthreads();
-    uint32_t* t = a;
-    a = b;
-    b = t;
+  for (uint32_t k = 0; k < kPer; ++k) {
+    const uint32_t i = k * kSortThreads + tid;
+    v[k] = (i < size) ? (uint32_t)src[off + i] - lo : 0xffffffffu;
   }
-  if (passes & 1) {
-    for (uint32_t i = tid; i < n; i += kSortThreads) b[i] = a[i];  // back into s.a
-    __syncthreads();
+#pragma unroll
+  for (uint32_t k = 0; k < kPer; ++k)
+    if (v[k] != 0xffffffffu) slot[k] = atomicAdd(&s.cnt[v[k] >> bshift], 1u);
+  __syncthreads();
+  // exclusive scan of the bucket counts (kBuckets / kSortThreads per thread)
+  constexpr uint32_t kBPer = kBuckets / kSortThreads;
+  uint32_t c[kBPer];
+  uint32_t tot = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kBPer; ++k) {
+    c[k] = s.cnt[tid * kBPer + k];
+    tot += c[k];
   }
+  uint32_t x = tot;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) s.wtot[wp] = x;
+  __syncthreads();
+  uint32_t run = x - tot;
+  for (uint32_t k = 0; k < wp; ++k) run += s.wtot[k];
+#pragma unroll
+  for (uint32_t k = 0; k < kBPer; ++k) {
+    s.base[tid * kBPer + k] = run;
+    run += c[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (uint32_t k = 0; k < kPer; ++k)
+    if (v[k] != 0xffffffffu) s.stage[s.base[v[k] >> bshift] + slot[k]] = v[k];
+  __syncthreads();
+  // insertion sort inside each bucket; then clear the counts
+#pragma unroll
+  for (uint32_t k = 0; k < kBPer; ++k) {
+    const uint32_t b = tid * kBPer + k;
+    const uint32_t b0 = s.base[b], n = c[k];
+    for (uint32_t i = 1; i < n; ++i) {
+      const uint32_t key = s.stage[b0 + i];
+      uint32_t j = i;
+      while (j > 0 && s.stage[b0 + j - 1] > key) {
+        s.stage[b0 + j] = s.stage[b0 + j - 1];
+        --j;
+      }
+      s.stage[b0 + j] = key;
+    }
+    s.cnt[b] = 0;
+  }
+  __syncthreads();
+  for (uint32_t i = tid; i < size; i += kSortThreads) __stcs(out + off + i, (int32_t)(s.stage[i] + lo));
+  __syncthreads();
 }
 
 __global__ void k_classify(const unsigned long long* __restrict__ offsets, uint32_t q, Job* small,
@@ -154,18 +150,16 @@ __global__ void k_classify(const unsigned long long* __restrict__ offsets, uint3
   }
 }
 
-// One CTA per small slice: load, radix sort on the low idbits, store.
+// One CTA per small slice (<= kSmallCap ids): bucket sort in shared memory.
 __global__ void __launch_bounds__(kSortThreads) k_sort_small(const Job* __restrict__ jobs, uint32_t njobs,
                                                              int32_t* out, uint32_t idbits) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  RadixSmem& s = *reinterpret_cast<RadixSmem*>(smem_raw);
+  BucketSmem& s = *reinterpret_cast<BucketSmem*>(smem_raw);
+  for (uint32_t i = threadIdx.x; i < kBuckets; i += kSortThreads) s.cnt[i] = 0;
+  __syncthreads();
   for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
     const Job jb = jobs[j];
-    for (uint32_t i = threadIdx.x; i < jb.size; i += kSortThreads) s.a[i] = (uint32_t)out[jb.off + i];
-    __syncthreads();
-    radix_sort_smem(s, jb.size, idbits);
-    for (uint32_t i = threadIdx.x; i < jb.size; i += kSortThreads) out[jb.off + i] = (int32_t)s.a[i];
-    __syncthreads();
+    bucket_sort_region(out, out, jb.off, jb.size, 0, idbits, s);
   }
 }
 
@@ -196,8 +190,15 @@ __global__ void __launch_bounds__(kTileThreads) k_win_hist(const Job* __restrict
     const Job jb = jobs[j];
     const uint32_t b0 = (t - tile_off[j]) * kTile;
     const uint32_t b1 = min(b0 + kTile, jb.size);
-    for (uint32_t i = b0 + threadIdx.x; i < b1; i += kTileThreads)
-      atomicAdd(&h[(uint32_t)src[jb.off + i] >> kWinBits], 1u);
+    uint32_t v[kTile / kTileThreads];
+#pragma unroll
+    for (uint32_t k = 0; k < kTile / kTileThreads; ++k) {
+      const uint32_t i = b0 + k * kTileThreads + threadIdx.x;
+      v[k] = (i < b1) ? (uint32_t)src[jb.off + i] : 0xffffffffu;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < kTile / kTileThreads; ++k)
+      if (v[k] != 0xffffffffu) atomicAdd(&h[v[k] >> kWinBits], 1u);
     __syncthreads();
     for (uint32_t w = threadIdx.x; w < G; w += kTileThreads)
       if (h[w]) atomicAdd(&whist[(size_t)j * G + w], h[w]);
@@ -265,10 +266,21 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
     const Job jb = jobs[j];
     const uint32_t b0 = (t - tile_off[j]) * kTile;
     const uint32_t n = min(b0 + kTile, jb.size) - b0;
-    for (uint32_t i = threadIdx.x; i < n; i += kTileThreads) {
-      const uint32_t id = (uint32_t)src[jb.off + b0 + i];
-      raw[i] = id;
-      atomicAdd(&cnt[id >> kWinBits], 1u);
+    {
+      uint32_t v[kTile / kTileThreads];
+#pragma unroll
+      for (uint32_t k = 0; k < kTile / kTileThreads; ++k) {
+        const uint32_t i = k * kTileThreads + threadIdx.x;
+        v[k] = (i < n) ? (uint32_t)__ldcs(src + jb.off + b0 + i) : 0xffffffffu;
+      }
+#pragma unroll
+      for (uint32_t k = 0; k < kTile / kTileThreads; ++k) {
+        const uint32_t i = k * kTileThreads + threadIdx.x;
+        if (i < n) {
+          raw[i] = v[k];
+          atomicAdd(&cnt[v[k] >> kWinBits], 1u);
+        }
+      }
     }
     __syncthreads();
     // exclusive scan of cnt -> lbase (each thread owns `per` consecutive windows)
@@ -313,14 +325,13 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
   }
 }
 
-// Persistent CTAs over the (job, window) regions: sort each window's ids
-// from src into out with a two-level bitmap in shared memory.  Insertion sets
-// the id's bit and the bit of its word in a summary bitmap; compaction gives
-// every thread one summary word (32 bitmap words), counts the ids under it,
-// takes its output position from a block scan and writes its ids in order,
-// clearing the words it read.  Work per region is proportional to its ids,
-// not to the window width.  With G == 1 the window is the whole slice and
-// src == out: all ids are inserted before any is written.
+// Persistent CTAs over the (job, window) regions.  Regions of at most
+// kSmallCap ids use the bucket sort.  Denser regions use a two-level bitmap:
+// insertion sets the id's bit and the bit of its word in a summary bitmap;
+// every thread then owns one summary word (32 bitmap words), counts the ids
+// under it, takes its output position from a block scan and writes its ids in
+// order, clearing the words it read.  With G == 1 the window is the whole
+// slice and src == out: all ids are read before any is written.
 __global__ void __launch_bounds__(kSortThreads) k_win_sort(
     const Job* __restrict__ jobs, uint32_t njobs, uint32_t G, uint32_t wbits,
     const uint32_t* __restrict__ whist, const unsigned long long* __restrict__ wbase,
@@ -328,6 +339,7 @@ __global__ void __launch_bounds__(kSortThreads) k_win_sort(
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint32_t* bm = reinterpret_cast<uint32_t*>(smem_raw);  // kBmWords
   uint32_t* sm = bm + kBmWords;                          // kSumWords
+  BucketSmem& bs = *reinterpret_cast<BucketSmem*>(smem_raw);
   __shared__ uint32_t wtot[kSortWarps];
   const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   const uint32_t nwords = ((1u << wbits) + 31) >> 5;
@@ -348,15 +360,31 @@ __global__ void __launch_bounds__(kSortThreads) k_win_sort(
     }
     if (size == 0) continue;
     const uint32_t lo = w << wbits;
-    if (size == 1) {
-      if (tid == 0) out[off] = src[off];
+    if (size <= kSmallCap) {
+      // bs.cnt aliases the (all-zero) bitmap, so it starts at zero
+      bucket_sort_region(src, out, off, size, lo, wbits, bs);
+      // its base/stage/wtot areas overlap the bitmap: zero what it wrote
+      for (uint32_t i = tid; i < kBuckets; i += kSortThreads) bs.base[i] = 0u;
+      for (uint32_t i = tid; i < size; i += kSortThreads) bs.stage[i] = 0u;
+      if (tid < kSortWarps) bs.wtot[tid] = 0u;
+      __syncthreads();
       continue;
     }
-    for (uint32_t i = tid; i < size; i += kSortThreads) {
-      const uint32_t rel = (uint32_t)src[off + i] - lo;
-      const uint32_t word = rel >> 5;
-      atomicOr(&bm[word], 1u << (rel & 31));
-      atomicOr(&sm[word >> 5], 1u << (word & 31));
+    for (uint32_t i0 = 0; i0 < size; i0 += kSortThreads * 8) {
+      uint32_t v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t i = i0 + k * kSortThreads + tid;
+        v[k] = (i < size) ? (uint32_t)__ldcs(src + off + i) : 0xffffffffu;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (v[k] == 0xffffffffu) continue;
+        const uint32_t rel = v[k] - lo;
+        const uint32_t word = rel >> 5;
+        atomicOr(&bm[word], 1u << (rel & 31));
+        atomicOr(&sm[word >> 5], 1u << (word & 31));
+      }
     }
     __syncthreads();
     const uint32_t s = (tid < nsum) ? sm[tid] : 0u;
@@ -395,6 +423,7 @@ qcp_status ws_reserve_sort(qcp_index* ix, Workspace* ws, size_t jobs, size_t til
 
 qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t s) {
   ws->sort_small_jobs = ws->sort_msd_jobs = 0;
+  ws->sort_part_marked = false;
   if (q == 0) return QCP_OK;
   uint32_t idbits = 1;
   while (idbits < 31 && (1ull << idbits) < ix->n) ++idbits;
@@ -402,8 +431,9 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   const uint32_t G = 1u << (idbits - wbits);
   const uint32_t sms = (uint32_t)num_sms();
 
-  const size_t radix_bytes = sizeof(RadixSmem);
-  const size_t win_bytes = sizeof(uint32_t) * (kBmWords + kSumWords);
+  const size_t radix_bytes = sizeof(BucketSmem);
+  const size_t bitmap_bytes = sizeof(uint32_t) * (kBmWords + kSumWords);
+  const size_t win_bytes = bitmap_bytes > sizeof(BucketSmem) ? bitmap_bytes : sizeof(BucketSmem);
   const size_t scatter_bytes = (size_t)G * 16 + kTile * 8;
   static thread_local int attrs_device = -1;  // attributes are per device
   if (attrs_device != ix->device) {
@@ -433,6 +463,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
     note_launch();
     QCP_TRY(check_launch("k_sort_small"));
   }
+  mark(ws, kEvSortSmall, s);
   if (nbig == 0) return QCP_OK;
 
   if (G == 1) {
@@ -480,6 +511,8 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
     k_win_scan<<<min(nbig, sms * 16), kTileThreads, 0, s>>>(big, nbig, G, whist, wbase, wcur);
     k_win_scatter<<<min(ntiles, sms * 8), kTileThreads, scatter_bytes, s>>>(big, map, tile_off, ntiles,
                                                                             ws->out_ids, ws->tmp_ids, G, wcur);
+    mark(ws, kEvSortPart, s);
+    ws->sort_part_marked = ws->timing;
     const uint64_t regions = (uint64_t)nbig * G;
     const uint32_t grid = (uint32_t)(regions < (uint64_t)sms * 3 ? regions : (uint64_t)sms * 3);
     k_win_sort<<<grid, kSortThreads, win_bytes, s>>>(big, nbig, G, wbits, whist, wbase, ws->tmp_ids,
