@@ -4,94 +4,84 @@
 // hits as ascending input ids.  The traversal writes each query's ids in
 // arbitrary order into its CSR slice; this file sorts every slice in place.
 // The ids of one slice are distinct and lie in [0, n), so only the low
-// `idbits` = ceil(log2 n) bits carry order, and a slice can be sorted by
-// setting one bit per id in a bitmap and reading the bitmap back in order.
+// `idbits` = ceil(log2 n) bits carry order.
 //
-//   slice <= kSmallCap ids   one 512-thread CTA bucket-sorts it in shared
-//                            memory: 2048 buckets by the top bits of the id,
-//                            atomic counts give every id a slot, a block scan
-//                            gives bucket bases, each bucket (a few ids) is
-//                            insertion-sorted, the order leaves coalesced.
-//   larger slices            1. window partition: ids are bucketed by
-//                               id >> kWinBits into G = 2^(idbits-kWinBits)
-//                               windows (tile histograms -> per-slice window
-//                               bases -> each tile regrouped by window in
-//                               shared memory and written as contiguous runs
-//                               into the scratch buffer);
-//                            2. persistent CTAs over the (slice, window)
-//                               regions: regions of <= kSmallCap ids are
-//                               bucket-sorted as above; denser ones set one
-//                               bit per id in a 64 KiB bitmap (plus a summary
-//                               bit per nonzero word) and compact it in
-//                               order.
-//                            With idbits <= kWinBits there is one window and
-//                            step 1 is skipped (the slice is sorted in place).
+// Every slice of more than one id is a job.  A job of at most kRegionCap ids
+// is one region, sorted in place.  A larger job is first split into
+// G = 2^g id windows (window = id >> (idbits - g), g chosen so that a window
+// holds about kTargetRegion ids): tile histograms -> per-window bases ->
+// every tile regrouped by window in shared memory and written as contiguous
+// runs into the scratch buffer.  Each window is then one region.
+//
+// A region is sorted by one CTA: ids are counted into 1024 buckets by their
+// top bits inside the region's id span (the atomic's return value is the
+// id's slot in its bucket), a block scan turns counts into bucket bases, ids
+// are placed into a shared staging array, each bucket (a few ids) is
+// insertion-sorted and the staged order leaves in coalesced stores.  A
+// region holding more than kRegionCap ids (ids clustered in id space) is
+// subdivided: its span is halved until each part fits, the parts are sorted
+// the same way and written in span order.
 #include "qcp_internal.cuh"
 
 namespace qcp {
 
 namespace {
 
-constexpr uint32_t kSmallCap = 8192;   // ids sorted by one CTA
-constexpr uint32_t kSortThreads = 512;
-constexpr uint32_t kSortWarps = kSortThreads / 32;
-constexpr uint32_t kWinBits = 19;      // 2^19 ids per window -> 64 KiB bitmap
-constexpr uint32_t kTile = 4096;       // ids per partition tile
+constexpr uint32_t kRegionCap = 8192;      // ids one CTA sorts at once
+constexpr uint32_t kTargetRegion = 4096;   // ids per window aimed at
+constexpr uint32_t kRegThreads = 256;
+constexpr uint32_t kRegWarps = kRegThreads / 32;
+constexpr uint32_t kBucketBits = 10;
+constexpr uint32_t kBuckets = 1u << kBucketBits;
+constexpr uint32_t kMaxG = 10;             // at most 2^10 windows per job
+constexpr uint32_t kTile = 4096;           // ids per partition tile
 constexpr uint32_t kTileThreads = 256;
-constexpr uint32_t kMaxWindows = 1u << (31 - kWinBits);
-constexpr uint32_t kBmWords = (1u << kWinBits) / 32;   // 16384 bitmap words
-constexpr uint32_t kSumWords = kBmWords / 32;           // 512 summary words
-constexpr uint32_t kBucketBits = 11;
-constexpr uint32_t kBuckets = 1u << kBucketBits;       // buckets of the region sort
 
 struct Job {
   unsigned long long off;
   uint32_t size;
-  uint32_t pad;
+  uint32_t g;  // log2 of the window count
 };
 
-// Shared memory of the bucket sort.
-struct BucketSmem {
-  uint32_t cnt[kBuckets];   // ids per bucket, then (after the scan) bucket ends
-  uint32_t base[kBuckets];  // first slot of each bucket
-  uint32_t stage[kSmallCap];
-  uint32_t wtot[kSortWarps];
+struct Region {
+  unsigned long long off;
+  uint32_t size;
+  uint32_t info;  // bit 0: ids in the scratch buffer; bits 1..5: span bits; bits 8..: window
 };
 
-// Sorts `size` (<= kSmallCap) distinct ids from src[off..) into out[off..)
-// (src may equal out: every id is read before any is written).  The ids lie
-// in [lo, lo + 2^wbits).  Bucket b holds ids whose offset from lo has b as
-// its top log2(kBuckets) bits; counting gives every id a slot in its bucket,
-// a block scan turns counts into bucket bases, each thread then
-// insertion-sorts the few ids of its buckets and the block copies the
-// staged order out with coalesced stores.  cnt[] must be zero on entry and
-// is zero again on exit.  Needs blockDim.x == kSortThreads.
-__device__ void bucket_sort_region(const int32_t* src, int32_t* out, unsigned long long off, uint32_t size,
-                                   uint32_t lo, uint32_t wbits, BucketSmem& s) {
+__device__ __forceinline__ uint32_t lanemask_lt_() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// Region sort
+// ---------------------------------------------------------------------------
+struct RegionSmem {
+  uint32_t cnt[kBuckets];
+  uint32_t base[kBuckets];
+  uint32_t stage[kRegionCap];
+  uint16_t slot[kRegionCap];
+  uint32_t wtot[kRegWarps];
+  uint32_t stack_lo[40];
+  uint32_t stack_bits[40];
+  uint32_t sp, count, pos;
+};
+
+// Block-wide exclusive scan of the bucket counts into base[] (kBuckets /
+// kRegThreads consecutive buckets per thread).
+__device__ __forceinline__ void scan_buckets(RegionSmem& s) {
+  constexpr uint32_t kPer = kBuckets / kRegThreads;
   const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-  const uint32_t bshift = wbits > kBucketBits ? wbits - kBucketBits : 0;
-  constexpr uint32_t kPer = kSmallCap / kSortThreads;  // 16 ids per thread at most
-  uint32_t v[kPer];
-  uint32_t slot[kPer];
+  uint32_t c[kPer];
+  uint32_t t = 0;
 #pragma unroll
   for (uint32_t k = 0; k < kPer; ++k) {
-    const uint32_t i = k * kSortThreads + tid;
-    v[k] = (i < size) ? (uint32_t)src[off + i] - lo : 0xffffffffu;
+    c[k] = s.cnt[tid * kPer + k];
+    t += c[k];
   }
-#pragma unroll
-  for (uint32_t k = 0; k < kPer; ++k)
-    if (v[k] != 0xffffffffu) slot[k] = atomicAdd(&s.cnt[v[k] >> bshift], 1u);
-  __syncthreads();
-  // exclusive scan of the bucket counts (kBuckets / kSortThreads per thread)
-  constexpr uint32_t kBPer = kBuckets / kSortThreads;
-  uint32_t c[kBPer];
-  uint32_t tot = 0;
-#pragma unroll
-  for (uint32_t k = 0; k < kBPer; ++k) {
-    c[k] = s.cnt[tid * kBPer + k];
-    tot += c[k];
-  }
-  uint32_t x = tot;
+  uint32_t x = t;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -99,23 +89,84 @@ __device__ void bucket_sort_region(const int32_t* src, int32_t* out, unsigned lo
   }
   if (lane == 31) s.wtot[wp] = x;
   __syncthreads();
-  uint32_t run = x - tot;
+  uint32_t run = x - t;
   for (uint32_t k = 0; k < wp; ++k) run += s.wtot[k];
 #pragma unroll
-  for (uint32_t k = 0; k < kBPer; ++k) {
-    s.base[tid * kBPer + k] = run;
+  for (uint32_t k = 0; k < kPer; ++k) {
+    s.base[tid * kPer + k] = run;
     run += c[k];
   }
   __syncthreads();
+}
+
+// Sorts the ids of src[off..off+size) that lie in [slo, slo + 2^sbits) --
+// exactly `count` (<= kRegionCap) of them -- into out[dst..dst+count).  With
+// filter == false every id of the range lies in the span (count == size).
+// s.cnt must be zero on entry; it is zero again on exit.
+__device__ void sort_span(const int32_t* src, unsigned long long off, uint32_t size, uint32_t slo,
+                          uint32_t sbits, bool filter, uint32_t count, int32_t* out,
+                          unsigned long long dst, RegionSmem& s) {
+  const uint32_t tid = threadIdx.x;
+  const uint32_t bshift = sbits > kBucketBits ? sbits - kBucketBits : 0;
+  const uint64_t span = 1ull << sbits;
+  if (!filter) {
+    // 1. count into buckets; each id's slot in its bucket is kept by index
+    for (uint32_t i0 = 0; i0 < size; i0 += kRegThreads * 8) {
+      uint32_t v[8];
 #pragma unroll
-  for (uint32_t k = 0; k < kPer; ++k)
-    if (v[k] != 0xffffffffu) s.stage[s.base[v[k] >> bshift] + slot[k]] = v[k];
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t i = i0 + k * kRegThreads + tid;
+        v[k] = (i < size) ? (uint32_t)src[off + i] - slo : 0xffffffffu;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t i = i0 + k * kRegThreads + tid;
+        if (v[k] != 0xffffffffu) s.slot[i] = (uint16_t)atomicAdd(&s.cnt[v[k] >> bshift], 1u);
+      }
+    }
+    __syncthreads();
+    scan_buckets(s);
+    // 2. place (the ids are read again, from L2)
+    for (uint32_t i0 = 0; i0 < size; i0 += kRegThreads * 8) {
+      uint32_t v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t i = i0 + k * kRegThreads + tid;
+        v[k] = (i < size) ? (uint32_t)src[off + i] - slo : 0xffffffffu;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t i = i0 + k * kRegThreads + tid;
+        if (v[k] != 0xffffffffu) s.stage[s.base[v[k] >> bshift] + s.slot[i]] = v[k];
+      }
+    }
+  } else {
+    // only the ids inside the span take part: count, scan, then place with
+    // a second round of atomics for the slots
+    for (uint32_t i = tid; i < size; i += kRegThreads) {
+      const uint32_t r = (uint32_t)src[off + i] - slo;
+      if ((uint64_t)r < span) atomicAdd(&s.cnt[r >> bshift], 1u);
+    }
+    __syncthreads();
+    scan_buckets(s);
+    for (uint32_t i = tid; i < kBuckets; i += kRegThreads) s.cnt[i] = 0;
+    __syncthreads();
+    for (uint32_t i = tid; i < size; i += kRegThreads) {
+      const uint32_t r = (uint32_t)src[off + i] - slo;
+      if ((uint64_t)r < span) {
+        const uint32_t b = r >> bshift;
+        s.stage[s.base[b] + atomicAdd(&s.cnt[b], 1u)] = r;
+      }
+    }
+  }
   __syncthreads();
-  // insertion sort inside each bucket; then clear the counts
+  // 3. insertion sort inside each bucket, clear the counts
+  constexpr uint32_t kPer = kBuckets / kRegThreads;
 #pragma unroll
-  for (uint32_t k = 0; k < kBPer; ++k) {
-    const uint32_t b = tid * kBPer + k;
-    const uint32_t b0 = s.base[b], n = c[k];
+  for (uint32_t k = 0; k < kPer; ++k) {
+    const uint32_t b = tid * kPer + k;
+    const uint32_t b0 = s.base[b];
+    const uint32_t n = s.cnt[b];
     for (uint32_t i = 1; i < n; ++i) {
       const uint32_t key = s.stage[b0 + i];
       uint32_t j = i;
@@ -128,12 +179,86 @@ __device__ void bucket_sort_region(const int32_t* src, int32_t* out, unsigned lo
     s.cnt[b] = 0;
   }
   __syncthreads();
-  for (uint32_t i = tid; i < size; i += kSortThreads) __stcs(out + off + i, (int32_t)(s.stage[i] + lo));
+  // 4. coalesced copy out
+  for (uint32_t i = tid; i < count; i += kRegThreads) __stcs(out + dst + i, (int32_t)(s.stage[i] + slo));
   __syncthreads();
 }
 
-__global__ void k_classify(const unsigned long long* __restrict__ offsets, uint32_t q, Job* small,
-                           uint32_t* nsmall, Job* big, uint32_t* nbig) {
+// Persistent CTAs over the regions.
+__global__ void __launch_bounds__(kRegThreads) k_region_sort(const Region* __restrict__ regions, uint32_t nreg,
+                                                             const int32_t* out_src, const int32_t* tmp_src,
+                                                             int32_t* out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RegionSmem& s = *reinterpret_cast<RegionSmem*>(smem_raw);
+  const uint32_t tid = threadIdx.x;
+  for (uint32_t i = tid; i < kBuckets; i += kRegThreads) s.cnt[i] = 0;
+  __syncthreads();
+  for (uint32_t r = blockIdx.x; r < nreg; r += gridDim.x) {
+    const Region rg = regions[r];
+    const int32_t* src = (rg.info & 1u) ? tmp_src : out_src;
+    const uint32_t sbits = (rg.info >> 1) & 31u;
+    const uint32_t lo = (rg.info >> 8) << sbits;
+    if (rg.size == 0) continue;
+    if (rg.size == 1) {
+      if (tid == 0) out[rg.off] = src[rg.off];
+      continue;
+    }
+    if (rg.size <= kRegionCap) {
+      sort_span(src, rg.off, rg.size, lo, sbits, false, rg.size, out, rg.off, s);
+      continue;
+    }
+    // more ids than one pass holds: halve the span until every part fits,
+    // emitting the parts in span order (only windows of split jobs get here,
+    // so src is the scratch buffer and out can be written while src is read)
+    if (tid == 0) {
+      s.sp = 1;
+      s.stack_lo[0] = lo;
+      s.stack_bits[0] = sbits;
+      s.pos = 0;
+    }
+    __syncthreads();
+    while (s.sp > 0) {
+      const uint32_t top = s.sp - 1;
+      const uint32_t slo = s.stack_lo[top], sb = s.stack_bits[top];
+      __syncthreads();
+      if (tid == 0) {
+        s.sp = top;
+        s.count = 0;
+      }
+      __syncthreads();
+      uint32_t c = 0;
+      const uint64_t span = 1ull << sb;
+      for (uint32_t i = tid; i < rg.size; i += kRegThreads)
+        c += ((uint64_t)((uint32_t)src[rg.off + i] - slo) < span) ? 1u : 0u;
+      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+      if ((tid & 31) == 0 && c) atomicAdd(&s.count, c);
+      __syncthreads();
+      const uint32_t count = s.count;
+      if (count > kRegionCap) {
+        if (tid == 0) {  // the upper half goes below the lower half on the stack
+          const uint32_t h = sb - 1;
+          s.stack_lo[s.sp] = slo + (1u << h);
+          s.stack_bits[s.sp] = h;
+          s.stack_lo[s.sp + 1] = slo;
+          s.stack_bits[s.sp + 1] = h;
+          s.sp += 2;
+        }
+      } else if (count > 0) {
+        sort_span(src, rg.off, rg.size, slo, sb, true, count, out, rg.off + s.pos, s);
+        if (tid == 0) s.pos += count;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Jobs and window partition
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t ceil_log2(uint32_t x) { return x <= 1 ? 0 : 32 - __clz(x - 1); }
+
+__global__ void k_classify(const unsigned long long* __restrict__ offsets, uint32_t q, uint32_t idbits,
+                           Job* jobs, uint32_t* njobs) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < q; i += gridDim.x * blockDim.x) {
     const unsigned long long off = offsets[i];
     const unsigned long long sz = offsets[i + 1] - off;
@@ -141,31 +266,23 @@ __global__ void k_classify(const unsigned long long* __restrict__ offsets, uint3
     Job j;
     j.off = off;
     j.size = (uint32_t)sz;
-    j.pad = 0;
-    if (sz <= kSmallCap) {
-      small[atomicAdd(nsmall, 1u)] = j;
-    } else {
-      big[atomicAdd(nbig, 1u)] = j;
+    uint32_t g = 0;
+    if (sz > kRegionCap) {
+      g = ceil_log2((uint32_t)((sz + kTargetRegion - 1) / kTargetRegion));
+      g = min(g, min(kMaxG, idbits));
     }
+    j.g = g;
+    jobs[atomicAdd(njobs, 1u)] = j;
   }
 }
 
-// One CTA per small slice (<= kSmallCap ids): bucket sort in shared memory.
-__global__ void __launch_bounds__(kSortThreads) k_sort_small(const Job* __restrict__ jobs, uint32_t njobs,
-                                                             int32_t* out, uint32_t idbits) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  BucketSmem& s = *reinterpret_cast<BucketSmem*>(smem_raw);
-  for (uint32_t i = threadIdx.x; i < kBuckets; i += kSortThreads) s.cnt[i] = 0;
-  __syncthreads();
-  for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
+// Per job: windows (1 for g == 0) and partition tiles (0 for g == 0).
+__global__ void k_job_counts(const Job* __restrict__ jobs, uint32_t njobs, uint32_t* nwin, uint32_t* ntile) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += gridDim.x * blockDim.x) {
     const Job jb = jobs[j];
-    bucket_sort_region(out, out, jb.off, jb.size, 0, idbits, s);
+    nwin[j] = 1u << jb.g;
+    ntile[j] = jb.g ? (jb.size + kTile - 1) / kTile : 0u;
   }
-}
-
-__global__ void k_tiles_per_job(const Job* __restrict__ jobs, uint32_t njobs, uint32_t* tiles) {
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += gridDim.x * blockDim.x)
-    tiles[j] = (jobs[j].size + kTile - 1) / kTile;
 }
 
 __global__ void k_tile_map(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ tile_off,
@@ -176,46 +293,71 @@ __global__ void k_tile_map(const uint32_t* __restrict__ tiles, const uint32_t* _
   }
 }
 
-// Window histogram of every tile -> whist[job][window].
+// Window histogram of every tile -> whist[woff[job] + window].
 __global__ void __launch_bounds__(kTileThreads) k_win_hist(const Job* __restrict__ jobs,
                                                            const uint32_t* __restrict__ map,
                                                            const uint32_t* __restrict__ tile_off,
                                                            uint32_t ntiles, const int32_t* __restrict__ src,
-                                                           uint32_t G, uint32_t* whist) {
-  extern __shared__ uint32_t h[];
+                                                           uint32_t idbits, const uint32_t* __restrict__ woff,
+                                                           uint32_t* whist) {
+  __shared__ uint32_t h[1u << kMaxG];
+  const uint32_t lane = threadIdx.x & 31;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    for (uint32_t w = threadIdx.x; w < G; w += kTileThreads) h[w] = 0;
-    __syncthreads();
     const uint32_t j = map[t];
     const Job jb = jobs[j];
+    const uint32_t G = 1u << jb.g;
+    const uint32_t shift = idbits - jb.g;
+    for (uint32_t w = threadIdx.x; w < G; w += kTileThreads) h[w] = 0;
+    __syncthreads();
     const uint32_t b0 = (t - tile_off[j]) * kTile;
     const uint32_t b1 = min(b0 + kTile, jb.size);
     uint32_t v[kTile / kTileThreads];
 #pragma unroll
     for (uint32_t k = 0; k < kTile / kTileThreads; ++k) {
       const uint32_t i = b0 + k * kTileThreads + threadIdx.x;
-      v[k] = (i < b1) ? (uint32_t)src[jb.off + i] : 0xffffffffu;
+      v[k] = (i < b1) ? (uint32_t)__ldcs(src + jb.off + i) : 0xffffffffu;
     }
 #pragma unroll
-    for (uint32_t k = 0; k < kTile / kTileThreads; ++k)
-      if (v[k] != 0xffffffffu) atomicAdd(&h[v[k] >> kWinBits], 1u);
+    for (uint32_t k = 0; k < kTile / kTileThreads; ++k) {
+      const bool valid = v[k] != 0xffffffffu;
+      const uint32_t active = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        const uint32_t w = v[k] >> shift;
+        const uint32_t peers = __match_any_sync(active, w);
+        if (lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&h[w], (uint32_t)__popc(peers));
+      }
+    }
     __syncthreads();
     for (uint32_t w = threadIdx.x; w < G; w += kTileThreads)
-      if (h[w]) atomicAdd(&whist[(size_t)j * G + w], h[w]);
+      if (h[w]) atomicAdd(&whist[woff[j] + w], h[w]);
     __syncthreads();
   }
 }
 
-// Per job: exclusive scan over its G window counts -> absolute bases and cursors.
+// Per job: exclusive scan over its window counts -> write cursors, and the
+// job's regions (one per window, or the whole slice for g == 0).
 __global__ void __launch_bounds__(kTileThreads) k_win_scan(const Job* __restrict__ jobs, uint32_t njobs,
-                                                           uint32_t G, const uint32_t* __restrict__ whist,
-                                                           unsigned long long* wbase,
-                                                           unsigned long long* wcur) {
+                                                           uint32_t idbits, const uint32_t* __restrict__ woff,
+                                                           const uint32_t* __restrict__ whist,
+                                                           unsigned long long* wcur, Region* regions) {
   __shared__ uint32_t wt[kTileThreads / 32];
-  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const uint32_t per = (G + kTileThreads - 1) / kTileThreads;  // consecutive windows per thread
+  const uint32_t lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
-    const size_t base = (size_t)j * G;
+    const Job jb = jobs[j];
+    const uint32_t base = woff[j];
+    if (jb.g == 0) {
+      if (threadIdx.x == 0) {
+        Region r;
+        r.off = jb.off;
+        r.size = jb.size;
+        r.info = (idbits << 1);  // ids in out, window 0, span = all ids
+        regions[base] = r;
+      }
+      continue;
+    }
+    const uint32_t G = 1u << jb.g;
+    const uint32_t sbits = idbits - jb.g;
+    const uint32_t per = (G + kTileThreads - 1) / kTileThreads;
     const uint32_t w0 = threadIdx.x * per;
     uint32_t s = 0;
     for (uint32_t k = 0; k < per; ++k)
@@ -226,16 +368,22 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scan(const Job* __restrict
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
       if (lane >= (uint32_t)o) x += y;
     }
-    if (lane == 31) wt[w] = x;
+    if (lane == 31) wt[wp] = x;
     __syncthreads();
     uint32_t before = 0;
-    for (uint32_t k = 0; k < w; ++k) before += wt[k];
-    unsigned long long run = jobs[j].off + before + x - s;
+    for (uint32_t k = 0; k < wp; ++k) before += wt[k];
+    unsigned long long run = jb.off + before + x - s;
     for (uint32_t k = 0; k < per; ++k) {
-      if (w0 + k < G) {
-        wbase[base + w0 + k] = run;
-        wcur[base + w0 + k] = run;
-        run += whist[base + w0 + k];
+      const uint32_t w = w0 + k;
+      if (w < G) {
+        const uint32_t c = whist[base + w];
+        wcur[base + w] = run;
+        Region r;
+        r.off = run;
+        r.size = c;
+        r.info = (w << 8) | (sbits << 1) | 1u;  // ids in the scratch buffer
+        regions[base + w] = r;
+        run += c;
       }
     }
     __syncthreads();
@@ -248,42 +396,50 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
                                                               const uint32_t* __restrict__ map,
                                                               const uint32_t* __restrict__ tile_off,
                                                               uint32_t ntiles, const int32_t* __restrict__ src,
-                                                              int32_t* __restrict__ dst, uint32_t G,
+                                                              int32_t* __restrict__ dst, uint32_t idbits,
+                                                              const uint32_t* __restrict__ woff,
                                                               unsigned long long* wcur) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned long long* gstart = reinterpret_cast<unsigned long long*>(smem_raw);   // G
-  uint32_t* cnt = reinterpret_cast<uint32_t*>(gstart + G);                        // G
-  uint32_t* lbase = cnt + G;                                                       // G
-  uint32_t* stage = lbase + G;                                                     // kTile
-  uint32_t* raw = stage + kTile;                                                   // kTile
+  __shared__ unsigned long long gstart[1u << kMaxG];
+  __shared__ uint32_t cnt[1u << kMaxG];
+  __shared__ uint32_t lbase[1u << kMaxG];
+  __shared__ uint32_t stage[kTile];
   __shared__ uint32_t wt[kTileThreads / 32];
   const uint32_t lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-  const uint32_t per = (G + kTileThreads - 1) / kTileThreads;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    for (uint32_t w = threadIdx.x; w < G; w += kTileThreads) cnt[w] = 0;
-    __syncthreads();
     const uint32_t j = map[t];
     const Job jb = jobs[j];
+    const uint32_t G = 1u << jb.g;
+    const uint32_t shift = idbits - jb.g;
+    for (uint32_t w = threadIdx.x; w < G; w += kTileThreads) cnt[w] = 0;
+    __syncthreads();
     const uint32_t b0 = (t - tile_off[j]) * kTile;
     const uint32_t n = min(b0 + kTile, jb.size) - b0;
-    {
-      uint32_t v[kTile / kTileThreads];
+    uint32_t v[kTile / kTileThreads];
+    uint32_t slot[kTile / kTileThreads];
 #pragma unroll
-      for (uint32_t k = 0; k < kTile / kTileThreads; ++k) {
-        const uint32_t i = k * kTileThreads + threadIdx.x;
-        v[k] = (i < n) ? (uint32_t)__ldcs(src + jb.off + b0 + i) : 0xffffffffu;
-      }
+    for (uint32_t k = 0; k < kTile / kTileThreads; ++k) {
+      const uint32_t i = k * kTileThreads + threadIdx.x;
+      v[k] = (i < n) ? (uint32_t)__ldcs(src + jb.off + b0 + i) : 0xffffffffu;
+    }
+    // slot of every id inside its window (warp-aggregated shared atomics)
 #pragma unroll
-      for (uint32_t k = 0; k < kTile / kTileThreads; ++k) {
-        const uint32_t i = k * kTileThreads + threadIdx.x;
-        if (i < n) {
-          raw[i] = v[k];
-          atomicAdd(&cnt[v[k] >> kWinBits], 1u);
-        }
+    for (uint32_t k = 0; k < kTile / kTileThreads; ++k) {
+      const bool valid = v[k] != 0xffffffffu;
+      const uint32_t active = __ballot_sync(0xffffffffu, valid);
+      slot[k] = 0;
+      if (valid) {
+        const uint32_t w = v[k] >> shift;
+        const uint32_t peers = __match_any_sync(active, w);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t b = 0;
+        if (lane == leader) b = atomicAdd(&cnt[w], (uint32_t)__popc(peers));
+        b = __shfl_sync(peers, b, leader);
+        slot[k] = b + __popc(peers & lanemask_lt_());
       }
     }
     __syncthreads();
-    // exclusive scan of cnt -> lbase (each thread owns `per` consecutive windows)
+    // exclusive scan of the window counts -> lbase; reserve global ranges
+    const uint32_t per = (G + kTileThreads - 1) / kTileThreads;
     const uint32_t w0 = threadIdx.x * per;
     uint32_t s = 0;
     for (uint32_t k = 0; k < per; ++k)
@@ -298,121 +454,25 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
     __syncthreads();
     uint32_t run = x - s;
     for (uint32_t k = 0; k < wp; ++k) run += wt[k];
-    __syncthreads();  // everyone has read wt before the next tile rewrites it
     for (uint32_t k = 0; k < per; ++k) {
       const uint32_t w = w0 + k;
       if (w < G) {
         const uint32_t c = cnt[w];
         lbase[w] = run;
-        if (c) gstart[w] = atomicAdd(&wcur[(size_t)j * G + w], (unsigned long long)c);
+        if (c) gstart[w] = atomicAdd(&wcur[woff[j] + w], (unsigned long long)c);
         run += c;
-        cnt[w] = 0;
       }
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += kTileThreads) {
-      const uint32_t id = raw[i];
-      const uint32_t w = id >> kWinBits;
-      stage[lbase[w] + atomicAdd(&cnt[w], 1u)] = id;
-    }
+#pragma unroll
+    for (uint32_t k = 0; k < kTile / kTileThreads; ++k)
+      if (v[k] != 0xffffffffu) stage[lbase[v[k] >> shift] + slot[k]] = v[k];
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < n; i += kTileThreads) {
       const uint32_t id = stage[i];
-      const uint32_t w = id >> kWinBits;
+      const uint32_t w = id >> shift;
       dst[gstart[w] + (i - lbase[w])] = (int32_t)id;
     }
-    __syncthreads();
-  }
-}
-
-// Persistent CTAs over the (job, window) regions.  Regions of at most
-// kSmallCap ids use the bucket sort.  Denser regions use a two-level bitmap:
-// insertion sets the id's bit and the bit of its word in a summary bitmap;
-// every thread then owns one summary word (32 bitmap words), counts the ids
-// under it, takes its output position from a block scan and writes its ids in
-// order, clearing the words it read.  With G == 1 the window is the whole
-// slice and src == out: all ids are read before any is written.
-__global__ void __launch_bounds__(kSortThreads) k_win_sort(
-    const Job* __restrict__ jobs, uint32_t njobs, uint32_t G, uint32_t wbits,
-    const uint32_t* __restrict__ whist, const unsigned long long* __restrict__ wbase,
-    const int32_t* src, int32_t* out) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint32_t* bm = reinterpret_cast<uint32_t*>(smem_raw);  // kBmWords
-  uint32_t* sm = bm + kBmWords;                          // kSumWords
-  BucketSmem& bs = *reinterpret_cast<BucketSmem*>(smem_raw);
-  __shared__ uint32_t wtot[kSortWarps];
-  const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-  const uint32_t nwords = ((1u << wbits) + 31) >> 5;
-  const uint32_t nsum = (nwords + 31) >> 5;  // <= kSortThreads
-  for (uint32_t i = tid; i < kBmWords + kSumWords; i += kSortThreads) bm[i] = 0u;
-  __syncthreads();
-  const uint64_t total = (uint64_t)njobs * G;
-  for (uint64_t g = blockIdx.x; g < total; g += gridDim.x) {
-    const uint32_t j = (uint32_t)(g / G), w = (uint32_t)(g % G);
-    uint32_t size;
-    unsigned long long off;
-    if (G == 1) {
-      size = jobs[j].size;
-      off = jobs[j].off;
-    } else {
-      size = whist[g];
-      off = wbase[g];
-    }
-    if (size == 0) continue;
-    const uint32_t lo = w << wbits;
-    if (size <= kSmallCap) {
-      // bs.cnt aliases the (all-zero) bitmap, so it starts at zero
-      bucket_sort_region(src, out, off, size, lo, wbits, bs);
-      // its base/stage/wtot areas overlap the bitmap: zero what it wrote
-      for (uint32_t i = tid; i < kBuckets; i += kSortThreads) bs.base[i] = 0u;
-      for (uint32_t i = tid; i < size; i += kSortThreads) bs.stage[i] = 0u;
-      if (tid < kSortWarps) bs.wtot[tid] = 0u;
-      __syncthreads();
-      continue;
-    }
-    for (uint32_t i0 = 0; i0 < size; i0 += kSortThreads * 8) {
-      uint32_t v[8];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const uint32_t i = i0 + k * kSortThreads + tid;
-        v[k] = (i < size) ? (uint32_t)__ldcs(src + off + i) : 0xffffffffu;
-      }
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if (v[k] == 0xffffffffu) continue;
-        const uint32_t rel = v[k] - lo;
-        const uint32_t word = rel >> 5;
-        atomicOr(&bm[word], 1u << (rel & 31));
-        atomicOr(&sm[word >> 5], 1u << (word & 31));
-      }
-    }
-    __syncthreads();
-    const uint32_t s = (tid < nsum) ? sm[tid] : 0u;
-    uint32_t c = 0;
-    for (uint32_t m = s; m; m &= m - 1) c += __popc(bm[tid * 32 + __ffs(m) - 1]);
-    uint32_t x = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= (uint32_t)o) x += y;
-    }
-    if (lane == 31) wtot[wp] = x;
-    __syncthreads();
-    uint32_t before = x - c;
-    for (uint32_t k = 0; k < wp; ++k) before += wtot[k];
-    unsigned long long o = off + before;
-    for (uint32_t m = s; m; m &= m - 1) {
-      const uint32_t wd = tid * 32 + __ffs(m) - 1;
-      uint32_t bits = bm[wd];
-      bm[wd] = 0u;
-      const uint32_t base_id = lo + (wd << 5);
-      while (bits) {
-        const int b = __ffs(bits) - 1;
-        bits &= bits - 1;
-        out[o++] = (int32_t)(base_id + (uint32_t)b);
-      }
-    }
-    if (tid < nsum) sm[tid] = 0u;
     __syncthreads();
   }
 }
@@ -427,102 +487,89 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   if (q == 0) return QCP_OK;
   uint32_t idbits = 1;
   while (idbits < 31 && (1ull << idbits) < ix->n) ++idbits;
-  const uint32_t wbits = idbits < kWinBits ? idbits : kWinBits;
-  const uint32_t G = 1u << (idbits - wbits);
   const uint32_t sms = (uint32_t)num_sms();
-
-  const size_t radix_bytes = sizeof(BucketSmem);
-  const size_t bitmap_bytes = sizeof(uint32_t) * (kBmWords + kSumWords);
-  const size_t win_bytes = bitmap_bytes > sizeof(BucketSmem) ? bitmap_bytes : sizeof(BucketSmem);
-  const size_t scatter_bytes = (size_t)G * 16 + kTile * 8;
+  const size_t region_bytes = sizeof(RegionSmem);
   static thread_local int attrs_device = -1;  // attributes are per device
   if (attrs_device != ix->device) {
-    QCP_CUDA(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)radix_bytes));
-    QCP_CUDA(cudaFuncSetAttribute(k_win_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)win_bytes));
-    QCP_CUDA(cudaFuncSetAttribute(k_win_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)((size_t)kMaxWindows * 16 + kTile * 8)));
+    QCP_CUDA(cudaFuncSetAttribute(k_region_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)region_bytes));
     attrs_device = ix->device;
   }
-
   QCP_TRY(ws_reserve_sort(ix, ws, (size_t)q + 256, 0));
   uint32_t* ctr = ws->ctr;
-  QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t) * 2, s));
-  Job* small = reinterpret_cast<Job*>(ws->jobs[0]);
-  Job* big = reinterpret_cast<Job*>(ws->jobs[1]);
-  k_classify<<<(q + 255) / 256, 256, 0, s>>>((const unsigned long long*)ws->offsets, q, small,
-                                             ctr + kCtrJobs0, big, ctr + kCtrJobs1);
+  QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t), s));
+  Job* jobs = reinterpret_cast<Job*>(ws->jobs[0]);
+  k_classify<<<(q + 255) / 256, 256, 0, s>>>((const unsigned long long*)ws->offsets, q, idbits, jobs,
+                                             ctr + kCtrJobs0);
   note_launch();
   QCP_CUDA(cudaMemcpyAsync(ws->h_ctr, ctr, sizeof(uint32_t) * kCtrCount, cudaMemcpyDeviceToHost, s));
   QCP_CUDA(cudaStreamSynchronize(s));
-  const uint32_t nsmall = ws->h_ctr[kCtrJobs0];
-  const uint32_t nbig = ws->h_ctr[kCtrJobs1];
-  ws->sort_small_jobs = nsmall;
-  ws->sort_msd_jobs = nbig;
-  if (nsmall) {
-    k_sort_small<<<min(nsmall, sms * 4), kSortThreads, radix_bytes, s>>>(small, nsmall, ws->out_ids, idbits);
-    note_launch();
-    QCP_TRY(check_launch("k_sort_small"));
-  }
-  mark(ws, kEvSortSmall, s);
-  if (nbig == 0) return QCP_OK;
+  const uint32_t njobs = ws->h_ctr[kCtrJobs0];
+  if (njobs == 0) return QCP_OK;
 
-  if (G == 1) {
-    k_win_sort<<<min(nbig, sms * 3), kSortThreads, win_bytes, s>>>(big, nbig, 1, wbits, nullptr, nullptr,
-                                                                   ws->out_ids, ws->out_ids);
-    note_launch();
-    return check_launch("k_win_sort");
-  }
-
-  // window partition tables: whist (u32), wbase, wcur (u64) per (job, window);
-  // tiles and tile offsets per job
-  const size_t nw = (size_t)nbig * G;
-  const size_t hist_bytes = (nw * 4 + 15) & ~(size_t)15;
-  const size_t bytes = hist_bytes + nw * 16 + (size_t)nbig * 8 + 64;
+  // per-job tables: windows, tiles and their offsets
+  const size_t tbytes = (size_t)njobs * 16 + 64;
   void* tables = nullptr;
-  QCP_TRY(ix->pool.get(bytes, &tables));
-  uint32_t* whist = reinterpret_cast<uint32_t*>(tables);
-  unsigned long long* wbase = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(tables) + hist_bytes);
-  unsigned long long* wcur = wbase + nw;
-  uint32_t* tiles = reinterpret_cast<uint32_t*>(wcur + nw);
-  uint32_t* tile_off = tiles + nbig;
+  QCP_TRY(ix->pool.get(tbytes, &tables));
+  uint32_t* nwin = reinterpret_cast<uint32_t*>(tables);
+  uint32_t* woff = nwin + njobs;
+  uint32_t* ntile = woff + njobs;
+  uint32_t* toff = ntile + njobs;
+  void* wtables = nullptr;
+  size_t wbytes = 0;
   qcp_status st = QCP_OK;
   do {
-    k_tiles_per_job<<<(nbig + 255) / 256, 256, 0, s>>>(big, nbig, tiles);
+    k_job_counts<<<(njobs + 255) / 256, 256, 0, s>>>(jobs, njobs, nwin, ntile);
     note_launch();
-    st = exclusive_scan<uint32_t>(tiles, tile_off, nbig, ctr + kCtrWork2, ix->pool, s);
-    if (st != QCP_OK) break;
-    if (cudaMemcpyAsync(ws->h_ctr + kCtrWork2, ctr + kCtrWork2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s) !=
-            cudaSuccess ||
+    if ((st = exclusive_scan<uint32_t>(nwin, woff, njobs, ctr + kCtrWork, ix->pool, s)) != QCP_OK) break;
+    if ((st = exclusive_scan<uint32_t>(ntile, toff, njobs, ctr + kCtrWork2, ix->pool, s)) != QCP_OK) break;
+    if (cudaMemcpyAsync(ws->h_ctr, ctr, sizeof(uint32_t) * kCtrCount, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess) {
-      st = cuda_status(cudaGetLastError(), "segmented sort tiles");
+      st = cuda_status(cudaGetLastError(), "segmented sort tables");
       break;
     }
+    const uint32_t nreg = ws->h_ctr[kCtrWork];
     const uint32_t ntiles = ws->h_ctr[kCtrWork2];
-    st = ws_reserve_sort(ix, ws, 0, ntiles);
-    if (st != QCP_OK) break;
-    uint32_t* map = ws->seg_hist;
-    k_tile_map<<<min(nbig, sms * 8), 256, 0, s>>>(tiles, tile_off, nbig, map);
-    if (cudaMemsetAsync(whist, 0, sizeof(uint32_t) * nw, s) != cudaSuccess) {
+    ws->sort_small_jobs = njobs;
+    ws->sort_msd_jobs = nreg;
+    // per-window tables: regions (16 B), cursors (u64), counts (u32)
+    wbytes = (size_t)nreg * (16 + 8 + 4) + 64;
+    if ((st = ix->pool.get(wbytes, &wtables)) != QCP_OK) {
+      wtables = nullptr;
+      break;
+    }
+    Region* regions = reinterpret_cast<Region*>(wtables);
+    unsigned long long* wcur = reinterpret_cast<unsigned long long*>(regions + nreg);
+    uint32_t* whist = reinterpret_cast<uint32_t*>(wcur + nreg);
+    if (cudaMemsetAsync(whist, 0, sizeof(uint32_t) * nreg, s) != cudaSuccess) {
       st = cuda_status(cudaGetLastError(), "memset");
       break;
     }
-    k_win_hist<<<min(ntiles, sms * 16), kTileThreads, sizeof(uint32_t) * G, s>>>(big, map, tile_off, ntiles,
-                                                                                 ws->out_ids, G, whist);
-    k_win_scan<<<min(nbig, sms * 16), kTileThreads, 0, s>>>(big, nbig, G, whist, wbase, wcur);
-    k_win_scatter<<<min(ntiles, sms * 8), kTileThreads, scatter_bytes, s>>>(big, map, tile_off, ntiles,
-                                                                            ws->out_ids, ws->tmp_ids, G, wcur);
+    mark(ws, kEvSortSmall, s);
+    if (ntiles) {
+      if ((st = ws_reserve_sort(ix, ws, 0, ntiles)) != QCP_OK) break;
+      k_tile_map<<<min(njobs, sms * 8), 256, 0, s>>>(ntile, toff, njobs, ws->seg_hist);
+      k_win_hist<<<min(ntiles, sms * 8), kTileThreads, 0, s>>>(jobs, ws->seg_hist, toff, ntiles, ws->out_ids,
+                                                              idbits, woff, whist);
+      note_launch(2);
+    }
+    k_win_scan<<<min(njobs, sms * 16), kTileThreads, 0, s>>>(jobs, njobs, idbits, woff, whist, wcur, regions);
+    note_launch();
+    if (ntiles) {
+      k_win_scatter<<<min(ntiles, sms * 4), kTileThreads, 0, s>>>(jobs, ws->seg_hist, toff, ntiles,
+                                                                 ws->out_ids, ws->tmp_ids, idbits, woff, wcur);
+      note_launch();
+    }
     mark(ws, kEvSortPart, s);
     ws->sort_part_marked = ws->timing;
-    const uint64_t regions = (uint64_t)nbig * G;
-    const uint32_t grid = (uint32_t)(regions < (uint64_t)sms * 3 ? regions : (uint64_t)sms * 3);
-    k_win_sort<<<grid, kSortThreads, win_bytes, s>>>(big, nbig, G, wbits, whist, wbase, ws->tmp_ids,
-                                                     ws->out_ids);
-    note_launch(5);
-    st = check_launch("segmented sort windows");
+    k_region_sort<<<min(nreg, sms * 4), kRegThreads, region_bytes, s>>>(regions, nreg, ws->out_ids,
+                                                                       ws->tmp_ids, ws->out_ids);
+    note_launch();
+    st = check_launch("segmented sort");
     // the tables go back to the pool below: make sure the kernels are done
     if (st == QCP_OK && cudaStreamSynchronize(s) != cudaSuccess) st = cuda_status(cudaGetLastError(), "sort");
   } while (false);
-  ix->pool.put(bytes, tables);
+  if (wtables) ix->pool.put(wbytes, wtables);
+  ix->pool.put(tbytes, tables);
   return st;
 }
 
