@@ -13,14 +13,16 @@
 // every tile regrouped by window in shared memory and written as contiguous
 // runs into the scratch buffer.  Each window is then one region.
 //
-// A region is sorted by one CTA: ids are counted into 1024 buckets by their
-// top bits inside the region's id span (the atomic's return value is the
-// id's slot in its bucket), a block scan turns counts into bucket bases, ids
-// are placed into a shared staging array, each bucket (a few ids) is
-// insertion-sorted and the staged order leaves in coalesced stores.  A
-// region holding more than kRegionCap ids (ids clustered in id space) is
-// subdivided: its span is halved until each part fits, the parts are sorted
-// the same way and written in span order.
+// A region is sorted by one CTA.  Windows at most 2^kSpanBits ids wide are
+// ranked through a bitmap: every id sets its bit, an exclusive popcount
+// prefix over the bitmap words gives each id its rank, ids are placed at
+// their rank in shared memory and leave in coalesced stores (no comparisons,
+// no divergence).  Wider spans (small slices of large id ranges) are counted
+// into 2048 buckets by their top bits (the atomic's return value is the id's
+// slot in its bucket), a block scan gives bucket bases, each bucket (a few
+// ids) is insertion-sorted.  A region holding more than kRegionCap ids (ids
+// clustered in id space) is subdivided: its span is halved until each part
+// fits, the parts are sorted by buckets and written in span order.
 #include "qcp_internal.cuh"
 
 namespace qcp {
@@ -28,14 +30,17 @@ namespace qcp {
 namespace {
 
 constexpr uint32_t kRegionCap = 8192;      // ids one CTA sorts at once
-constexpr uint32_t kTargetRegion = 4096;   // ids per window aimed at
+constexpr uint32_t kTargetRegion = 6144;   // ids per window aimed at
 constexpr uint32_t kRegThreads = 256;
 constexpr uint32_t kRegWarps = kRegThreads / 32;
-constexpr uint32_t kBucketBits = 10;
+constexpr uint32_t kBucketBits = 11;
 constexpr uint32_t kBuckets = 1u << kBucketBits;
+constexpr uint32_t kSpanBits = 17;         // widest window the bitmap path takes
+constexpr uint32_t kBmWords = (1u << kSpanBits) / 32;  // 4096
 constexpr uint32_t kMaxG = 10;             // at most 2^10 windows per job
 constexpr uint32_t kTile = 4096;           // ids per partition tile
 constexpr uint32_t kTileThreads = 256;
+constexpr uint32_t kTileWarps = kTileThreads / 32;
 
 struct Job {
   unsigned long long off;
@@ -49,20 +54,22 @@ struct Region {
   uint32_t info;  // bit 0: ids in the scratch buffer; bits 1..5: span bits; bits 8..: window
 };
 
-__device__ __forceinline__ uint32_t lanemask_lt_() {
-  uint32_t m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
-
 // ---------------------------------------------------------------------------
 // Region sort
 // ---------------------------------------------------------------------------
 struct RegionSmem {
-  uint32_t cnt[kBuckets];
-  uint32_t base[kBuckets];
-  uint32_t stage[kRegionCap];
-  uint16_t slot[kRegionCap];
+  uint32_t stage[kRegionCap];  // sorted ids on their way out
+  union {
+    struct {  // bucket path
+      uint32_t cnt[kBuckets];
+      uint32_t base[kBuckets];
+      uint16_t slot[kRegionCap];
+    } bk;
+    struct {  // bitmap path
+      uint32_t bm[kBmWords];
+      uint32_t pre[kBmWords];  // exclusive popcount prefix per word
+    } bmp;
+  };
   uint32_t wtot[kRegWarps];
   uint32_t stack_lo[40];
   uint32_t stack_bits[40];
@@ -78,7 +85,7 @@ __device__ __forceinline__ void scan_buckets(RegionSmem& s) {
   uint32_t t = 0;
 #pragma unroll
   for (uint32_t k = 0; k < kPer; ++k) {
-    c[k] = s.cnt[tid * kPer + k];
+    c[k] = s.bk.cnt[tid * kPer + k];
     t += c[k];
   }
   uint32_t x = t;
@@ -93,7 +100,7 @@ __device__ __forceinline__ void scan_buckets(RegionSmem& s) {
   for (uint32_t k = 0; k < wp; ++k) run += s.wtot[k];
 #pragma unroll
   for (uint32_t k = 0; k < kPer; ++k) {
-    s.base[tid * kPer + k] = run;
+    s.bk.base[tid * kPer + k] = run;
     run += c[k];
   }
   __syncthreads();
@@ -121,7 +128,7 @@ __device__ void sort_span(const int32_t* src, unsigned long long off, uint32_t s
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const uint32_t i = i0 + k * kRegThreads + tid;
-        if (v[k] != 0xffffffffu) s.slot[i] = (uint16_t)atomicAdd(&s.cnt[v[k] >> bshift], 1u);
+        if (v[k] != 0xffffffffu) s.bk.slot[i] = (uint16_t)atomicAdd(&s.bk.cnt[v[k] >> bshift], 1u);
       }
     }
     __syncthreads();
@@ -137,7 +144,7 @@ __device__ void sort_span(const int32_t* src, unsigned long long off, uint32_t s
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const uint32_t i = i0 + k * kRegThreads + tid;
-        if (v[k] != 0xffffffffu) s.stage[s.base[v[k] >> bshift] + s.slot[i]] = v[k];
+        if (v[k] != 0xffffffffu) s.stage[s.bk.base[v[k] >> bshift] + s.bk.slot[i]] = v[k];
       }
     }
   } else {
@@ -145,17 +152,17 @@ __device__ void sort_span(const int32_t* src, unsigned long long off, uint32_t s
     // a second round of atomics for the slots
     for (uint32_t i = tid; i < size; i += kRegThreads) {
       const uint32_t r = (uint32_t)src[off + i] - slo;
-      if ((uint64_t)r < span) atomicAdd(&s.cnt[r >> bshift], 1u);
+      if ((uint64_t)r < span) atomicAdd(&s.bk.cnt[r >> bshift], 1u);
     }
     __syncthreads();
     scan_buckets(s);
-    for (uint32_t i = tid; i < kBuckets; i += kRegThreads) s.cnt[i] = 0;
+    for (uint32_t i = tid; i < kBuckets; i += kRegThreads) s.bk.cnt[i] = 0;
     __syncthreads();
     for (uint32_t i = tid; i < size; i += kRegThreads) {
       const uint32_t r = (uint32_t)src[off + i] - slo;
       if ((uint64_t)r < span) {
         const uint32_t b = r >> bshift;
-        s.stage[s.base[b] + atomicAdd(&s.cnt[b], 1u)] = r;
+        s.stage[s.bk.base[b] + atomicAdd(&s.bk.cnt[b], 1u)] = r;
       }
     }
   }
@@ -165,8 +172,8 @@ __device__ void sort_span(const int32_t* src, unsigned long long off, uint32_t s
 #pragma unroll
   for (uint32_t k = 0; k < kPer; ++k) {
     const uint32_t b = tid * kPer + k;
-    const uint32_t b0 = s.base[b];
-    const uint32_t n = s.cnt[b];
+    const uint32_t b0 = s.bk.base[b];
+    const uint32_t n = s.bk.cnt[b];
     for (uint32_t i = 1; i < n; ++i) {
       const uint32_t key = s.stage[b0 + i];
       uint32_t j = i;
@@ -176,11 +183,96 @@ __device__ void sort_span(const int32_t* src, unsigned long long off, uint32_t s
       }
       s.stage[b0 + j] = key;
     }
-    s.cnt[b] = 0;
+    s.bk.cnt[b] = 0;
   }
   __syncthreads();
   // 4. coalesced copy out
   for (uint32_t i = tid; i < count; i += kRegThreads) __stcs(out + dst + i, (int32_t)(s.stage[i] + slo));
+  __syncthreads();
+}
+
+// Sorts the `size` (<= kRegionCap) distinct ids of src[off..) -- all in
+// [lo, lo + 2^sbits), sbits <= kSpanBits -- into out[off..) by rank: every id
+// sets its bit in a bitmap of the span, an exclusive popcount prefix over the
+// bitmap words gives the number of smaller ids before each word, so an id's
+// rank is pre[word] + popc(word & bits below it).  No id is compared and no
+// thread diverges.  The bucket counters (which share this memory) are zero
+// on entry and zero again on exit.
+__device__ void sort_span_bitmap(const int32_t* src, unsigned long long off, uint32_t size, uint32_t lo,
+                                 uint32_t sbits, int32_t* out, RegionSmem& s) {
+  const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  const uint32_t nwords = ((1u << sbits) + 31) >> 5;           // <= kBmWords
+  constexpr uint32_t kPer = kBmWords / kRegThreads;            // 16 words per thread
+  uint4* bm4 = reinterpret_cast<uint4*>(s.bmp.bm);
+  for (uint32_t i = tid; i < kBmWords / 4; i += kRegThreads) bm4[i] = make_uint4(0, 0, 0, 0);
+  __syncthreads();
+  for (uint32_t i0 = 0; i0 < size; i0 += kRegThreads * 8) {
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t i = i0 + k * kRegThreads + tid;
+      v[k] = (i < size) ? (uint32_t)src[off + i] - lo : 0xffffffffu;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (v[k] != 0xffffffffu) atomicOr(&s.bmp.bm[v[k] >> 5], 1u << (v[k] & 31));
+  }
+  __syncthreads();
+  // exclusive popcount prefix: each thread owns kPer consecutive words
+  uint32_t c[kPer];
+  uint32_t t = 0;
+  const uint32_t w0 = tid * kPer;
+#pragma unroll
+  for (uint32_t k = 0; k < kPer; k += 4) {
+    const uint4 q = (w0 + k < nwords) ? bm4[(w0 + k) / 4] : make_uint4(0, 0, 0, 0);
+    c[k] = __popc(q.x);
+    c[k + 1] = __popc(q.y);
+    c[k + 2] = __popc(q.z);
+    c[k + 3] = __popc(q.w);
+    t += c[k] + c[k + 1] + c[k + 2] + c[k + 3];
+  }
+  uint32_t x = t;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) s.wtot[wp] = x;
+  __syncthreads();
+  uint32_t run = x - t;
+  for (uint32_t k = 0; k < wp; ++k) run += s.wtot[k];
+  uint4* pre4 = reinterpret_cast<uint4*>(s.bmp.pre);
+#pragma unroll
+  for (uint32_t k = 0; k < kPer; k += 4) {
+    uint4 q;
+    q.x = run;
+    q.y = q.x + c[k];
+    q.z = q.y + c[k + 1];
+    q.w = q.z + c[k + 2];
+    run = q.w + c[k + 3];
+    pre4[(w0 + k) / 4] = q;
+  }
+  __syncthreads();
+  // rank and place (ids read again, from L2)
+  for (uint32_t i0 = 0; i0 < size; i0 += kRegThreads * 8) {
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t i = i0 + k * kRegThreads + tid;
+      v[k] = (i < size) ? (uint32_t)src[off + i] - lo : 0xffffffffu;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (v[k] == 0xffffffffu) continue;
+      const uint32_t w = v[k] >> 5;
+      const uint32_t below = s.bmp.bm[w] & ((1u << (v[k] & 31)) - 1u);
+      s.stage[s.bmp.pre[w] + __popc(below)] = v[k];
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = tid; i < size; i += kRegThreads) __stcs(out + off + i, (int32_t)(s.stage[i] + lo));
+  // restore the zero bucket counters that alias the bitmap
+  for (uint32_t i = tid; i < kBuckets; i += kRegThreads) s.bk.cnt[i] = 0;
   __syncthreads();
 }
 
@@ -191,7 +283,7 @@ __global__ void __launch_bounds__(kRegThreads) k_region_sort(const Region* __res
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RegionSmem& s = *reinterpret_cast<RegionSmem*>(smem_raw);
   const uint32_t tid = threadIdx.x;
-  for (uint32_t i = tid; i < kBuckets; i += kRegThreads) s.cnt[i] = 0;
+  for (uint32_t i = tid; i < kBuckets; i += kRegThreads) s.bk.cnt[i] = 0;
   __syncthreads();
   for (uint32_t r = blockIdx.x; r < nreg; r += gridDim.x) {
     const Region rg = regions[r];
@@ -204,7 +296,10 @@ __global__ void __launch_bounds__(kRegThreads) k_region_sort(const Region* __res
       continue;
     }
     if (rg.size <= kRegionCap) {
-      sort_span(src, rg.off, rg.size, lo, sbits, false, rg.size, out, rg.off, s);
+      if (sbits <= kSpanBits)
+        sort_span_bitmap(src, rg.off, rg.size, lo, sbits, out, s);
+      else
+        sort_span(src, rg.off, rg.size, lo, sbits, false, rg.size, out, rg.off, s);
       continue;
     }
     // more ids than one pass holds: halve the span until every part fits,
@@ -268,7 +363,9 @@ __global__ void k_classify(const unsigned long long* __restrict__ offsets, uint3
     j.size = (uint32_t)sz;
     uint32_t g = 0;
     if (sz > kRegionCap) {
+      // windows narrow enough for the bitmap path and small enough to fit
       g = ceil_log2((uint32_t)((sz + kTargetRegion - 1) / kTargetRegion));
+      if (idbits > kSpanBits) g = max(g, idbits - kSpanBits);
       g = min(g, min(kMaxG, idbits));
     }
     j.g = g;
@@ -293,21 +390,22 @@ __global__ void k_tile_map(const uint32_t* __restrict__ tiles, const uint32_t* _
   }
 }
 
-// Window histogram of every tile -> whist[woff[job] + window].
+// Window histogram of every tile -> whist[woff[job] + window].  Each warp
+// counts into its own shared counters (no contention across warps).
 __global__ void __launch_bounds__(kTileThreads) k_win_hist(const Job* __restrict__ jobs,
                                                            const uint32_t* __restrict__ map,
                                                            const uint32_t* __restrict__ tile_off,
                                                            uint32_t ntiles, const int32_t* __restrict__ src,
                                                            uint32_t idbits, const uint32_t* __restrict__ woff,
                                                            uint32_t* whist) {
-  __shared__ uint32_t h[1u << kMaxG];
-  const uint32_t lane = threadIdx.x & 31;
+  extern __shared__ uint32_t h[];  // [kTileWarps][G]
+  const uint32_t wp = threadIdx.x >> 5;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const uint32_t j = map[t];
     const Job jb = jobs[j];
     const uint32_t G = 1u << jb.g;
     const uint32_t shift = idbits - jb.g;
-    for (uint32_t w = threadIdx.x; w < G; w += kTileThreads) h[w] = 0;
+    for (uint32_t w = threadIdx.x; w < G * kTileWarps; w += kTileThreads) h[w] = 0;
     __syncthreads();
     const uint32_t b0 = (t - tile_off[j]) * kTile;
     const uint32_t b1 = min(b0 + kTile, jb.size);
@@ -317,19 +415,16 @@ __global__ void __launch_bounds__(kTileThreads) k_win_hist(const Job* __restrict
       const uint32_t i = b0 + k * kTileThreads + threadIdx.x;
       v[k] = (i < b1) ? (uint32_t)__ldcs(src + jb.off + i) : 0xffffffffu;
     }
+    uint32_t* hw = h + wp * G;
 #pragma unroll
-    for (uint32_t k = 0; k < kTile / kTileThreads; ++k) {
-      const bool valid = v[k] != 0xffffffffu;
-      const uint32_t active = __ballot_sync(0xffffffffu, valid);
-      if (valid) {
-        const uint32_t w = v[k] >> shift;
-        const uint32_t peers = __match_any_sync(active, w);
-        if (lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&h[w], (uint32_t)__popc(peers));
-      }
-    }
+    for (uint32_t k = 0; k < kTile / kTileThreads; ++k)
+      if (v[k] != 0xffffffffu) atomicAdd(&hw[v[k] >> shift], 1u);
     __syncthreads();
-    for (uint32_t w = threadIdx.x; w < G; w += kTileThreads)
-      if (h[w]) atomicAdd(&whist[woff[j] + w], h[w]);
+    for (uint32_t w = threadIdx.x; w < G; w += kTileThreads) {
+      uint32_t c = 0;
+      for (uint32_t k = 0; k < kTileWarps; ++k) c += h[k * G + w];
+      if (c) atomicAdd(&whist[woff[j] + w], c);
+    }
     __syncthreads();
   }
 }
@@ -391,7 +486,10 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scan(const Job* __restrict
 }
 
 // Each tile: regroup its ids by window in shared memory, reserve the window
-// ranges with one atomic per nonempty window, write contiguous runs.
+// ranges with one atomic per nonempty window, write contiguous runs.  Each
+// warp counts into its own shared counters; the counter's old value is the
+// id's slot among its warp's ids of that window (the order inside a window
+// does not matter, the region sort orders it).
 __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restrict__ jobs,
                                                               const uint32_t* __restrict__ map,
                                                               const uint32_t* __restrict__ tile_off,
@@ -399,9 +497,10 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
                                                               int32_t* __restrict__ dst, uint32_t idbits,
                                                               const uint32_t* __restrict__ woff,
                                                               unsigned long long* wcur) {
-  __shared__ unsigned long long gstart[1u << kMaxG];
-  __shared__ uint32_t cnt[1u << kMaxG];
-  __shared__ uint32_t lbase[1u << kMaxG];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned long long* gstart = reinterpret_cast<unsigned long long*>(smem_raw);  // [G]
+  uint32_t* lbase = reinterpret_cast<uint32_t*>(gstart + (1u << kMaxG));       // [G]
+  uint32_t* cnt = lbase + (1u << kMaxG);                                        // [kTileWarps][G]
   __shared__ uint32_t stage[kTile];
   __shared__ uint32_t wt[kTileThreads / 32];
   const uint32_t lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
@@ -410,7 +509,7 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
     const Job jb = jobs[j];
     const uint32_t G = 1u << jb.g;
     const uint32_t shift = idbits - jb.g;
-    for (uint32_t w = threadIdx.x; w < G; w += kTileThreads) cnt[w] = 0;
+    for (uint32_t w = threadIdx.x; w < G * kTileWarps; w += kTileThreads) cnt[w] = 0;
     __syncthreads();
     const uint32_t b0 = (t - tile_off[j]) * kTile;
     const uint32_t n = min(b0 + kTile, jb.size) - b0;
@@ -421,29 +520,21 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
       const uint32_t i = k * kTileThreads + threadIdx.x;
       v[k] = (i < n) ? (uint32_t)__ldcs(src + jb.off + b0 + i) : 0xffffffffu;
     }
-    // slot of every id inside its window (warp-aggregated shared atomics)
+    uint32_t* cw = cnt + wp * G;
 #pragma unroll
-    for (uint32_t k = 0; k < kTile / kTileThreads; ++k) {
-      const bool valid = v[k] != 0xffffffffu;
-      const uint32_t active = __ballot_sync(0xffffffffu, valid);
-      slot[k] = 0;
-      if (valid) {
-        const uint32_t w = v[k] >> shift;
-        const uint32_t peers = __match_any_sync(active, w);
-        const uint32_t leader = __ffs(peers) - 1;
-        uint32_t b = 0;
-        if (lane == leader) b = atomicAdd(&cnt[w], (uint32_t)__popc(peers));
-        b = __shfl_sync(peers, b, leader);
-        slot[k] = b + __popc(peers & lanemask_lt_());
-      }
-    }
+    for (uint32_t k = 0; k < kTile / kTileThreads; ++k)
+      slot[k] = (v[k] != 0xffffffffu) ? atomicAdd(&cw[v[k] >> shift], 1u) : 0u;
     __syncthreads();
-    // exclusive scan of the window counts -> lbase; reserve global ranges
+    // per window: exclusive scan over (window, warp) -> each warp's base in
+    // the tile's window-grouped order; window totals reserve global ranges
     const uint32_t per = (G + kTileThreads - 1) / kTileThreads;
     const uint32_t w0 = threadIdx.x * per;
     uint32_t s = 0;
-    for (uint32_t k = 0; k < per; ++k)
-      if (w0 + k < G) s += cnt[w0 + k];
+    for (uint32_t k = 0; k < per; ++k) {
+      const uint32_t w = w0 + k;
+      if (w < G)
+        for (uint32_t q = 0; q < kTileWarps; ++q) s += cnt[q * G + w];
+    }
     uint32_t x = s;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -457,16 +548,21 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
     for (uint32_t k = 0; k < per; ++k) {
       const uint32_t w = w0 + k;
       if (w < G) {
-        const uint32_t c = cnt[w];
         lbase[w] = run;
-        if (c) gstart[w] = atomicAdd(&wcur[woff[j] + w], (unsigned long long)c);
-        run += c;
+        uint32_t tot = 0;
+        for (uint32_t q = 0; q < kTileWarps; ++q) {
+          const uint32_t c = cnt[q * G + w];
+          cnt[q * G + w] = run + tot;  // now: this warp's first slot in the tile
+          tot += c;
+        }
+        if (tot) gstart[w] = atomicAdd(&wcur[woff[j] + w], (unsigned long long)tot);
+        run += tot;
       }
     }
     __syncthreads();
 #pragma unroll
     for (uint32_t k = 0; k < kTile / kTileThreads; ++k)
-      if (v[k] != 0xffffffffu) stage[lbase[v[k] >> shift] + slot[k]] = v[k];
+      if (v[k] != 0xffffffffu) stage[cw[v[k] >> shift] + slot[k]] = v[k];
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < n; i += kTileThreads) {
       const uint32_t id = stage[i];
@@ -489,9 +585,13 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   while (idbits < 31 && (1ull << idbits) < ix->n) ++idbits;
   const uint32_t sms = (uint32_t)num_sms();
   const size_t region_bytes = sizeof(RegionSmem);
+  const size_t hist_bytes = sizeof(uint32_t) * kTileWarps * (1u << kMaxG);
+  const size_t scatter_bytes = (sizeof(unsigned long long) + sizeof(uint32_t) * (1 + kTileWarps)) * (1u << kMaxG);
   static thread_local int attrs_device = -1;  // attributes are per device
   if (attrs_device != ix->device) {
     QCP_CUDA(cudaFuncSetAttribute(k_region_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)region_bytes));
+    QCP_CUDA(cudaFuncSetAttribute(k_win_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_bytes));
+    QCP_CUDA(cudaFuncSetAttribute(k_win_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_bytes));
     attrs_device = ix->device;
   }
   QCP_TRY(ws_reserve_sort(ix, ws, (size_t)q + 256, 0));
@@ -548,15 +648,15 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
     if (ntiles) {
       if ((st = ws_reserve_sort(ix, ws, 0, ntiles)) != QCP_OK) break;
       k_tile_map<<<min(njobs, sms * 8), 256, 0, s>>>(ntile, toff, njobs, ws->seg_hist);
-      k_win_hist<<<min(ntiles, sms * 8), kTileThreads, 0, s>>>(jobs, ws->seg_hist, toff, ntiles, ws->out_ids,
-                                                              idbits, woff, whist);
+      k_win_hist<<<min(ntiles, sms * 8), kTileThreads, hist_bytes, s>>>(jobs, ws->seg_hist, toff, ntiles,
+                                                                       ws->out_ids, idbits, woff, whist);
       note_launch(2);
     }
     k_win_scan<<<min(njobs, sms * 16), kTileThreads, 0, s>>>(jobs, njobs, idbits, woff, whist, wcur, regions);
     note_launch();
     if (ntiles) {
-      k_win_scatter<<<min(ntiles, sms * 4), kTileThreads, 0, s>>>(jobs, ws->seg_hist, toff, ntiles,
-                                                                 ws->out_ids, ws->tmp_ids, idbits, woff, wcur);
+      k_win_scatter<<<min(ntiles, sms * 4), kTileThreads, scatter_bytes, s>>>(
+          jobs, ws->seg_hist, toff, ntiles, ws->out_ids, ws->tmp_ids, idbits, woff, wcur);
       note_launch();
     }
     mark(ws, kEvSortPart, s);
