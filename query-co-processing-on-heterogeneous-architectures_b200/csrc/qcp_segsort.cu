@@ -19,14 +19,13 @@
 //                              tile regrouped by window in shared memory and
 //                              written as contiguous runs into the scratch
 //                              buffer;
-//                           2. each (slice, window) is ranked through a
-//                              bitmap of its 2^wbits possible ids: every id
-//                              sets its bit, an exclusive popcount prefix
-//                              over the bitmap gives each id its rank, ids
-//                              are placed at their rank in shared memory and
-//                              leave in coalesced stores -- no comparisons,
-//                              no divergence.  The next window's ids are
-//                              loaded while the current one is ranked.
+//                           2. each (slice, window) is sorted with a
+//                              two-level bitmap of its 2^wbits possible ids
+//                              (one bit per id plus one summary bit per
+//                              nonzero word): ids set their bits, then each
+//                              thread compacts the words under one summary
+//                              word, in order, at the position a block scan
+//                              of the per-thread counts gives it.
 #include "qcp_internal.cuh"
 
 namespace qcp {
@@ -45,13 +44,10 @@ constexpr uint32_t kTile = 4096;
 constexpr uint32_t kTileThreads = 256;
 constexpr uint32_t kTileWarps = kTileThreads / 32;
 constexpr uint32_t kPerWarpMaxG = 256;  // per-warp window counters up to this G
-// ---- window ranking ---------------------------------------------------------
+// ---- window sort ------------------------------------------------------------
 constexpr uint32_t kRankThreads = 512;
 constexpr uint32_t kRankWarps = kRankThreads / 32;
 constexpr uint32_t kBmWords = (1u << kWinBits) / 32;  // 16384
-constexpr uint32_t kPreGroups = kBmWords / 4;          // prefix per 4 words
-constexpr uint32_t kStage = 8192;                      // ranked ids per pass
-constexpr uint32_t kHeld = kStage / kRankThreads;      // ids held per thread: 16
 
 struct Job {
   unsigned long long off;
@@ -342,159 +338,85 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
 }
 
 // ============================================================================
-// Window ranking
+// Window sort
 // ============================================================================
-struct RankSmem {
-  uint32_t bm[kBmWords];       // one bit per possible id of the window
-  uint32_t pre[kPreGroups];    // ids before each group of 4 words
-  uint32_t stage[kStage];      // ranked ids on their way out
-  uint32_t wtot[kRankWarps];
-};
+constexpr uint32_t kSumWords = kBmWords / 32;  // 512 summary words
 
-// Rank of id offset r (its bit set in bm) among the window's ids.
-__device__ __forceinline__ uint32_t rank_of(const RankSmem& s, uint32_t r) {
-  const uint32_t w = r >> 5;
-  const uint4 g = reinterpret_cast<const uint4*>(s.bm)[w >> 2];
-  uint32_t k = s.pre[w >> 2];
-  const uint32_t sub = w & 3;
-  const uint32_t mask = (1u << (r & 31)) - 1u;
-  if (sub == 0) {
-    k += __popc(g.x & mask);
-  } else if (sub == 1) {
-    k += __popc(g.x) + __popc(g.y & mask);
-  } else if (sub == 2) {
-    k += __popc(g.x) + __popc(g.y) + __popc(g.z & mask);
-  } else {
-    k += __popc(g.x) + __popc(g.y) + __popc(g.z) + __popc(g.w & mask);
-  }
-  return k;
-}
-
-// Persistent CTAs over the (job, window) pairs g = job * G + window.  The ids
-// of window g are read from src (the scratch buffer) and written, ranked, to
-// out.  While a window is ranked its successor's ids are already in flight
-// into registers (windows of at most kStage ids; the ids of larger ones
-// beyond the first kStage are read again where needed).
-__global__ void __launch_bounds__(kRankThreads, 2) k_win_rank(uint64_t total, uint32_t G, uint32_t wbits,
-                                                              const uint32_t* __restrict__ whist,
-                                                              const unsigned long long* __restrict__ wbase,
-                                                              const int32_t* __restrict__ src,
-                                                              int32_t* __restrict__ out) {
+// Persistent CTAs over the (job, window) pairs g = job * G + window: sort each
+// window's ids from src (the scratch buffer) into out with a two-level bitmap
+// in shared memory.  Insertion sets the id's bit and the bit of its word in a
+// summary bitmap; compaction gives every thread one summary word (32 bitmap
+// words), counts the ids under it, takes its output position from a block
+// scan and writes its ids in order, clearing the words it read.  The work per
+// window follows its ids, not the window width.
+__global__ void __launch_bounds__(kRankThreads) k_win_sort(uint64_t total, uint32_t G, uint32_t wbits,
+                                                           const uint32_t* __restrict__ whist,
+                                                           const unsigned long long* __restrict__ wbase,
+                                                           const int32_t* __restrict__ src,
+                                                           int32_t* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  RankSmem& s = *reinterpret_cast<RankSmem*>(smem_raw);
+  uint32_t* bm = reinterpret_cast<uint32_t*>(smem_raw);  // kBmWords
+  uint32_t* sm = bm + kBmWords;                          // kSumWords
+  __shared__ uint32_t wtot[kRankWarps];
   const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   const uint32_t nwords = ((1u << wbits) + 31) >> 5;
-  const uint32_t ngroups = (nwords + 3) >> 2;
-  uint4* bm4 = reinterpret_cast<uint4*>(s.bm);
-  for (uint32_t i = tid; i < kBmWords / 4; i += kRankThreads) bm4[i] = make_uint4(0, 0, 0, 0);
+  const uint32_t nsum = (nwords + 31) >> 5;  // <= kRankThreads
+  for (uint32_t i = tid; i < kBmWords + kSumWords; i += kRankThreads) bm[i] = 0u;
   __syncthreads();
-
-  uint64_t g = blockIdx.x;
-  uint32_t size = 0;
-  unsigned long long off = 0;
-  uint32_t held[kHeld];
-#pragma unroll
-  for (uint32_t k = 0; k < kHeld; ++k) held[k] = 0xffffffffu;
-  if (g < total) {
-    size = whist[g];
-    off = wbase[g];
-#pragma unroll
-    for (uint32_t k = 0; k < kHeld; ++k) {
-      const uint32_t i = k * kRankThreads + tid;
-      held[k] = (i < size) ? (uint32_t)__ldcs(src + off + i) : 0xffffffffu;
-    }
-  }
-  while (g < total) {
+  for (uint64_t g = blockIdx.x; g < total; g += gridDim.x) {
+    const uint32_t size = whist[g];
+    const unsigned long long off = wbase[g];
+    if (size == 0) continue;
     const uint32_t lo = (uint32_t)(g % G) << wbits;
-    // the next window's size and offset
-    const uint64_t gn = g + gridDim.x;
-    uint32_t size_n = 0;
-    unsigned long long off_n = 0;
-    if (gn < total) {
-      size_n = whist[gn];
-      off_n = wbase[gn];
+    if (size == 1) {
+      if (tid == 0) out[off] = src[off];
+      continue;
     }
-    if (size > 0) {
-      // 1. set bits (the held ids, then any beyond kStage)
+    // 8 independent loads in flight per thread before the shared atomics
+    for (uint32_t i0 = 0; i0 < size; i0 += kRankThreads * 8) {
+      uint32_t v[8];
 #pragma unroll
-      for (uint32_t k = 0; k < kHeld; ++k)
-        if (held[k] != 0xffffffffu) {
-          const uint32_t r = held[k] - lo;
-          atomicOr(&s.bm[r >> 5], 1u << (r & 31));
-        }
-      for (uint32_t i = kStage + tid; i < size; i += kRankThreads) {
-        const uint32_t r = (uint32_t)src[off + i] - lo;
-        atomicOr(&s.bm[r >> 5], 1u << (r & 31));
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t i = i0 + k * kRankThreads + tid;
+        v[k] = (i < size) ? (uint32_t)__ldcs(src + off + i) : 0xffffffffu;
       }
-      __syncthreads();
-      // 2. exclusive popcount prefix per group of 4 words
-      constexpr uint32_t kGPer = kPreGroups / kRankThreads;  // 8 groups per thread
-      uint32_t c[kGPer];
-      uint32_t t = 0;
 #pragma unroll
-      for (uint32_t k = 0; k < kGPer; ++k) {
-        const uint32_t gi = tid * kGPer + k;
-        uint32_t pc = 0;
-        if (gi < ngroups) {
-          const uint4 q = bm4[gi];
-          pc = __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
-        }
-        c[k] = pc;
-        t += pc;
+      for (int k = 0; k < 8; ++k) {
+        if (v[k] == 0xffffffffu) continue;
+        const uint32_t rel = v[k] - lo;
+        const uint32_t word = rel >> 5;
+        atomicOr(&bm[word], 1u << (rel & 31));
+        atomicOr(&sm[word >> 5], 1u << (word & 31));
       }
-      uint32_t x = t;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= (uint32_t)o) x += y;
-      }
-      if (lane == 31) s.wtot[wp] = x;
-      __syncthreads();
-      uint32_t run = x - t;
-      for (uint32_t k = 0; k < wp; ++k) run += s.wtot[k];
-#pragma unroll
-      for (uint32_t k = 0; k < kGPer; ++k) {
-        s.pre[tid * kGPer + k] = run;
-        run += c[k];
-      }
-      __syncthreads();
-      // 3. place by rank and write out, kStage ranks per pass
-      for (uint32_t p0 = 0; p0 < size; p0 += kStage) {
-        const uint32_t p1 = min(p0 + kStage, size);
-#pragma unroll
-        for (uint32_t k = 0; k < kHeld; ++k)
-          if (held[k] != 0xffffffffu) {
-            const uint32_t r = held[k] - lo;
-            const uint32_t rk = rank_of(s, r);
-            if (rk >= p0 && rk < p1) s.stage[rk - p0] = r;
-          }
-        for (uint32_t i = kStage + tid; i < size; i += kRankThreads) {
-          const uint32_t r = (uint32_t)src[off + i] - lo;
-          const uint32_t rk = rank_of(s, r);
-          if (rk >= p0 && rk < p1) s.stage[rk - p0] = r;
-        }
-        __syncthreads();
-        for (uint32_t i = tid; i < p1 - p0; i += kRankThreads)
-          __stcs(out + off + p0 + i, (int32_t)(s.stage[i] + lo));
-        __syncthreads();
-      }
-      // 4. clear the bitmap words that were set
-#pragma unroll
-      for (uint32_t k = 0; k < kHeld; ++k)
-        if (held[k] != 0xffffffffu) s.bm[(held[k] - lo) >> 5] = 0u;
-      for (uint32_t i = kStage + tid; i < size; i += kRankThreads)
-        s.bm[((uint32_t)src[off + i] - lo) >> 5] = 0u;
-    }
-    // 5. the next window's ids, in flight across the barrier
-#pragma unroll
-    for (uint32_t k = 0; k < kHeld; ++k) {
-      const uint32_t i = k * kRankThreads + tid;
-      held[k] = (gn < total && i < size_n) ? (uint32_t)__ldcs(src + off_n + i) : 0xffffffffu;
     }
     __syncthreads();
-    g = gn;
-    size = size_n;
-    off = off_n;
+    const uint32_t sw = (tid < nsum) ? sm[tid] : 0u;
+    uint32_t c = 0;
+    for (uint32_t m = sw; m; m &= m - 1) c += __popc(bm[tid * 32 + __ffs(m) - 1]);
+    uint32_t x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) wtot[wp] = x;
+    __syncthreads();
+    uint32_t before = x - c;
+    for (uint32_t k = 0; k < wp; ++k) before += wtot[k];
+    unsigned long long o = off + before;
+    for (uint32_t m = sw; m; m &= m - 1) {
+      const uint32_t wd = tid * 32 + __ffs(m) - 1;
+      uint32_t bits = bm[wd];
+      bm[wd] = 0u;
+      const uint32_t base_id = lo + (wd << 5);
+      while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        out[o++] = (int32_t)(base_id + (uint32_t)b);
+      }
+    }
+    if (tid < nsum) sm[tid] = 0u;
+    __syncthreads();
   }
 }
 
@@ -512,14 +434,14 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   const uint32_t G = 1u << (idbits - wbits);
   const uint32_t sms = (uint32_t)num_sms();
   const size_t small_bytes = sizeof(BucketSmem);
-  const size_t rank_bytes = sizeof(RankSmem);
+  const size_t rank_bytes = sizeof(uint32_t) * (kBmWords + kSumWords);
   const uint32_t nsets = (G <= kPerWarpMaxG) ? kTileWarps : 1u;
   const size_t scatter_bytes = (size_t)G * (8 + 4 + 4 * nsets) + kTile * 4;
   const size_t scatter_max = (size_t)(1u << (31 - kWinBits)) * 16 + kTile * 4;
   static thread_local int attrs_device = -1;  // attributes are per device
   if (attrs_device != ix->device) {
     QCP_CUDA(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_bytes));
-    QCP_CUDA(cudaFuncSetAttribute(k_win_rank, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rank_bytes));
+    QCP_CUDA(cudaFuncSetAttribute(k_win_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rank_bytes));
     QCP_CUDA(cudaFuncSetAttribute(k_win_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(scatter_max > scatter_bytes ? scatter_max : scatter_bytes)));
     attrs_device = ix->device;
@@ -588,8 +510,8 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
                                                                             wcur);
     mark(ws, kEvSortPart, s);
     ws->sort_part_marked = ws->timing;
-    const uint32_t grid = (uint32_t)(nw < (uint64_t)sms * 2 ? nw : (uint64_t)sms * 2);
-    k_win_rank<<<grid, kRankThreads, rank_bytes, s>>>(nw, G, wbits, whist, wbase, ws->tmp_ids, ws->out_ids);
+    const uint32_t grid = (uint32_t)(nw < (uint64_t)sms * 3 ? nw : (uint64_t)sms * 3);
+    k_win_sort<<<grid, kRankThreads, rank_bytes, s>>>(nw, G, wbits, whist, wbase, ws->tmp_ids, ws->out_ids);
     note_launch(5);
     st = check_launch("segmented sort windows");
     // the tables go back to the pool below: make sure the kernels are done
