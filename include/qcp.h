@@ -179,6 +179,22 @@ qcp_status qcp_index_load(const char* path, void* stream, qcp_index** out);
 qcp_status qcp_index_export(const qcp_index* index, uint64_t* keys, int32_t* ids,
                             uint32_t level, float* mbr);
 
+/* Hit count of each of q (<= 262144) queries, computed by the batched
+ * traversal, without allocating any memory -- for callers that must not call
+ * cudaMalloc while they query (device memory owned by another allocator,
+ * serving loops that cannot take cudaMalloc's implicit synchronisation,
+ * allocation only at start-up by policy).  d_boxes (q rows of 2*dims floats)
+ * and d_counts (q entries) are device memory the caller owns.  The
+ * traversal's scratch is one fixed array of about 20 MiB in the library's
+ * device image, held by every GPU that loads the library until exit and
+ * shared by all calls: calls that overlap on the GPU race and must be
+ * serialised by the caller.  The first call on a device looks up the
+ * array's device address; make it before any stream capture.  A batch whose
+ * traversal frontier exceeds the scratch returns QCP_ERR_OUTPUT_OVERFLOW
+ * (split the batch).  No counterpart in the reference. */
+qcp_status qcp_query_counts_noalloc(qcp_index* index, const float* d_boxes, uint32_t q,
+                                    uint64_t* d_counts, void* stream);
+
 /* Message of the last error on the calling host thread ("" if none). */
 const char* qcp_last_error(void);
 

@@ -251,6 +251,9 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
 qcp_status run_plain(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_only, bool sort,
                      cudaStream_t s);
 qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t s);
+qcp_status run_batched_counts_into(qcp_index* ix, const float* boxes, uint32_t q, uint64_t* counts,
+                                   uint2* items0, uint2* items1, uint32_t* item_hits, size_t item_cap,
+                                   uint32_t* ctr, unsigned long long* stats, cudaStream_t s);
 qcp_status exclusive_scan_counts(const uint64_t* counts, uint64_t* offsets, uint32_t q,
                                  DevPool& pool, cudaStream_t s);
 template <class T>

@@ -581,4 +581,48 @@ qcp_status run_plain(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_only,
   return QCP_OK;
 }
 
+// Batched per-query hit counts into caller-provided device buffers (boxes,
+// counts) with scratch supplied by the caller as well: two frontier buffers
+// of item_cap items, item_cap per-item counts, kCtrCount counters and
+// kStatCount statistics words.  Nothing is allocated.  Returns
+// QCP_ERR_OUTPUT_OVERFLOW when the batch's frontier exceeds item_cap.
+qcp_status run_batched_counts_into(qcp_index* ix, const float* boxes, uint32_t q, uint64_t* counts,
+                                   uint2* items0, uint2* items1, uint32_t* item_hits, size_t item_cap,
+                                   uint32_t* ctr, unsigned long long* stats, cudaStream_t s) {
+  const TreeView t = view_of(ix);
+  const uint32_t D = ix->dims;
+  const bool rect = ix->is_rect != 0;
+  const uint32_t grid = (uint32_t)num_sms() * 8;
+  uint2* items[2] = {items0, items1};
+  const uint32_t start = (ix->levels >= 2) ? ix->levels - 1 : 1;
+  QCP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * kCtrCount, s));
+  QCP_CUDA(cudaMemsetAsync(stats, 0, sizeof(unsigned long long) * kStatCount, s));
+  QCP_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint64_t) * q, s));
+  k_init_items<<<(q + 255) / 256, 256, 0, s>>>(items[0], q, 0, ctr + kCtrFrontier0);
+  note_launch();
+  int cur = 0;
+  for (uint32_t l = start; l > 1; --l) {
+    const int nxt = cur ^ 1;
+    QCP_CUDA(cudaMemsetAsync(ctr + kCtrFrontier0 + nxt, 0, sizeof(uint32_t), s));
+    QCP_DISPATCH_D(D, launch_expand<DD>(grid, s, boxes, items[cur], ctr + kCtrFrontier0 + cur, items[nxt],
+                                        ctr + kCtrFrontier0 + nxt, item_cap, t.mbr[l - 1], t.nodes[l - 1],
+                                        t.pad[l - 1], t.fanout, ctr + kCtrOverflow, ctr + kCtrNeedItems));
+    note_launch();
+    cur = nxt;
+  }
+  QCP_DISPATCH_D(D, launch_leafscan<DD, kCount>(rect, grid, s, t, boxes, items[cur], ctr + kCtrFrontier0 + cur,
+                                                ctr + kCtrWork, item_hits, counts, nullptr, nullptr, nullptr,
+                                                item_cap, stats));
+  note_launch();
+  QCP_TRY(check_launch("batched counts"));
+  uint32_t overflow = 0;  // pageable host word: no pinned buffer is allocated
+  QCP_CUDA(cudaMemcpyAsync(&overflow, ctr + kCtrOverflow, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  QCP_CUDA(cudaStreamSynchronize(s));
+  if (overflow) {
+    set_error("query frontier exceeds the fixed scratch of this entry point; split the batch");
+    return QCP_ERR_OUTPUT_OVERFLOW;
+  }
+  return QCP_OK;
+}
+
 }  // namespace qcp
