@@ -19,13 +19,13 @@
 //                              tile regrouped by window in shared memory and
 //                              written as contiguous runs into the scratch
 //                              buffer;
-//                           2. each (slice, window) is sorted with a
-//                              two-level bitmap of its 2^wbits possible ids
-//                              (one bit per id plus one summary bit per
-//                              nonzero word): ids set their bits, then each
-//                              thread compacts the words under one summary
-//                              word, in order, at the position a block scan
-//                              of the per-thread counts gives it.
+//                           2. each (slice, window) is ranked through a
+//                              bitmap of its 2^wbits possible ids: every id
+//                              sets its bit, an exclusive popcount prefix
+//                              over groups of bitmap words gives each id its
+//                              rank, ids are placed at their rank in shared
+//                              memory and leave in coalesced stores -- no
+//                              comparisons, no divergence.
 #include "qcp_internal.cuh"
 
 namespace qcp {
@@ -340,82 +340,133 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
 // ============================================================================
 // Window sort
 // ============================================================================
-constexpr uint32_t kSumWords = kBmWords / 32;  // 512 summary words
+constexpr uint32_t kGroups = kBmWords / 4;             // 4096 groups of 4 words
+constexpr uint32_t kGroupsPer = kGroups / kRankThreads; // 8 per thread
+constexpr uint32_t kStage = 8192;                      // ranked ids staged in smem
 
-// Persistent CTAs over the (job, window) pairs g = job * G + window: sort each
-// window's ids from src (the scratch buffer) into out with a two-level bitmap
-// in shared memory.  Insertion sets the id's bit and the bit of its word in a
-// summary bitmap; compaction gives every thread one summary word (32 bitmap
-// words), counts the ids under it, takes its output position from a block
-// scan and writes its ids in order, clearing the words it read.  The work per
-// window follows its ids, not the window width.
-__global__ void __launch_bounds__(kRankThreads) k_win_sort(uint64_t total, uint32_t G, uint32_t wbits,
-                                                           const uint32_t* __restrict__ whist,
-                                                           const unsigned long long* __restrict__ wbase,
-                                                           const int32_t* __restrict__ src,
-                                                           int32_t* __restrict__ out) {
+struct RankSmem {
+  uint32_t bm[kBmWords];     // one bit per possible id of the window
+  uint32_t pre[kGroups];     // ids before each group of 4 words
+  uint32_t stage[kStage];    // ranks [0, kStage) on their way out
+  uint32_t wtot[kRankWarps];
+};
+
+// Rank of id offset r among the window's ids: the ids before r's group plus
+// the set bits below r inside the group (branch-free).
+__device__ __forceinline__ uint32_t rank_in(const RankSmem& s, uint32_t r) {
+  const uint32_t w = r >> 5;
+  const uint32_t sub = w & 3u;
+  const uint4 q = reinterpret_cast<const uint4*>(s.bm)[w >> 2];
+  const uint32_t below = (1u << (r & 31u)) - 1u;
+  const uint32_t m0 = sub > 0 ? 0xffffffffu : below;
+  const uint32_t m1 = sub > 1 ? 0xffffffffu : (sub == 1 ? below : 0u);
+  const uint32_t m2 = sub > 2 ? 0xffffffffu : (sub == 2 ? below : 0u);
+  const uint32_t m3 = sub == 3 ? below : 0u;
+  return s.pre[w >> 2] + __popc(q.x & m0) + __popc(q.y & m1) + __popc(q.z & m2) + __popc(q.w & m3);
+}
+
+// Persistent CTAs over the (job, window) pairs g = job * G + window: the ids
+// of window g (from src, the scratch buffer) are ranked through a bitmap of
+// the window's 2^wbits possible ids -- every id sets its bit, an exclusive
+// popcount prefix over groups of 4 bitmap words gives each id its rank --
+// placed at their rank in shared memory and written out in coalesced stores.
+// No comparisons, no divergence; the groups that were set are cleared from
+// the prefix pass's counts.
+__global__ void __launch_bounds__(kRankThreads, 2) k_win_sort(uint32_t total, uint32_t G, uint32_t wbits,
+                                                              const uint32_t* __restrict__ whist,
+                                                              const unsigned long long* __restrict__ wbase,
+                                                              const int32_t* __restrict__ src,
+                                                              int32_t* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint32_t* bm = reinterpret_cast<uint32_t*>(smem_raw);  // kBmWords
-  uint32_t* sm = bm + kBmWords;                          // kSumWords
-  __shared__ uint32_t wtot[kRankWarps];
+  RankSmem& s = *reinterpret_cast<RankSmem*>(smem_raw);
   const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-  const uint32_t nwords = ((1u << wbits) + 31) >> 5;
-  const uint32_t nsum = (nwords + 31) >> 5;  // <= kRankThreads
-  for (uint32_t i = tid; i < kBmWords + kSumWords; i += kRankThreads) bm[i] = 0u;
+  uint4* bm4 = reinterpret_cast<uint4*>(s.bm);
+  for (uint32_t i = tid; i < kGroups; i += kRankThreads) bm4[i] = make_uint4(0, 0, 0, 0);
   __syncthreads();
-  for (uint64_t g = blockIdx.x; g < total; g += gridDim.x) {
+  for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
     const uint32_t size = whist[g];
-    const unsigned long long off = wbase[g];
     if (size == 0) continue;
-    const uint32_t lo = (uint32_t)(g % G) << wbits;
+    const unsigned long long off = wbase[g];
+    const int32_t* in = src + off;
+    int32_t* dst = out + off;
+    const uint32_t lo = (g % G) << wbits;
     if (size == 1) {
-      if (tid == 0) out[off] = src[off];
+      if (tid == 0) dst[0] = in[0];
       continue;
     }
-    // 8 independent loads in flight per thread before the shared atomics
-    for (uint32_t i0 = 0; i0 < size; i0 += kRankThreads * 8) {
-      uint32_t v[8];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const uint32_t i = i0 + k * kRankThreads + tid;
-        v[k] = (i < size) ? (uint32_t)__ldcs(src + off + i) : 0xffffffffu;
-      }
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if (v[k] == 0xffffffffu) continue;
-        const uint32_t rel = v[k] - lo;
-        const uint32_t word = rel >> 5;
-        atomicOr(&bm[word], 1u << (rel & 31));
-        atomicOr(&sm[word >> 5], 1u << (word & 31));
-      }
+    // 1. set one bit per id
+    uint32_t i = tid;
+    for (; i + 3 * kRankThreads < size; i += 4 * kRankThreads) {
+      const uint32_t a = (uint32_t)__ldcg(in + i) - lo, b = (uint32_t)__ldcg(in + i + kRankThreads) - lo;
+      const uint32_t c = (uint32_t)__ldcg(in + i + 2 * kRankThreads) - lo;
+      const uint32_t d = (uint32_t)__ldcg(in + i + 3 * kRankThreads) - lo;
+      atomicOr(&s.bm[a >> 5], 1u << (a & 31));
+      atomicOr(&s.bm[b >> 5], 1u << (b & 31));
+      atomicOr(&s.bm[c >> 5], 1u << (c & 31));
+      atomicOr(&s.bm[d >> 5], 1u << (d & 31));
+    }
+    for (; i < size; i += kRankThreads) {
+      const uint32_t a = (uint32_t)__ldcg(in + i) - lo;
+      atomicOr(&s.bm[a >> 5], 1u << (a & 31));
     }
     __syncthreads();
-    const uint32_t sw = (tid < nsum) ? sm[tid] : 0u;
-    uint32_t c = 0;
-    for (uint32_t m = sw; m; m &= m - 1) c += __popc(bm[tid * 32 + __ffs(m) - 1]);
-    uint32_t x = c;
+    // 2. exclusive popcount prefix over groups (kGroupsPer consecutive per thread)
+    uint32_t c[kGroupsPer];
+    uint32_t t = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < kGroupsPer; ++k) {
+      const uint4 q = bm4[tid * kGroupsPer + k];
+      c[k] = __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
+      t += c[k];
+    }
+    uint32_t x = t;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
       if (lane >= (uint32_t)o) x += y;
     }
-    if (lane == 31) wtot[wp] = x;
+    if (lane == 31) s.wtot[wp] = x;
     __syncthreads();
-    uint32_t before = x - c;
-    for (uint32_t k = 0; k < wp; ++k) before += wtot[k];
-    unsigned long long o = off + before;
-    for (uint32_t m = sw; m; m &= m - 1) {
-      const uint32_t wd = tid * 32 + __ffs(m) - 1;
-      uint32_t bits = bm[wd];
-      bm[wd] = 0u;
-      const uint32_t base_id = lo + (wd << 5);
-      while (bits) {
-        const int b = __ffs(bits) - 1;
-        bits &= bits - 1;
-        out[o++] = (int32_t)(base_id + (uint32_t)b);
+    uint32_t run = x - t;
+    for (uint32_t k = 0; k < wp; ++k) run += s.wtot[k];
+#pragma unroll
+    for (uint32_t k = 0; k < kGroupsPer; ++k) {
+      s.pre[tid * kGroupsPer + k] = run;
+      run += c[k];
+    }
+    __syncthreads();
+    // 3. rank every id (read again, from L2); ranks past kStage go straight out
+    i = tid;
+    for (; i + 3 * kRankThreads < size; i += 4 * kRankThreads) {
+      uint32_t r[4];
+      r[0] = (uint32_t)__ldcs(in + i) - lo;
+      r[1] = (uint32_t)__ldcs(in + i + kRankThreads) - lo;
+      r[2] = (uint32_t)__ldcs(in + i + 2 * kRankThreads) - lo;
+      r[3] = (uint32_t)__ldcs(in + i + 3 * kRankThreads) - lo;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint32_t rk = rank_in(s, r[k]);
+        if (rk < kStage)
+          s.stage[rk] = r[k];
+        else
+          __stcs(dst + rk, (int32_t)(r[k] + lo));
       }
     }
-    if (tid < nsum) sm[tid] = 0u;
+    for (; i < size; i += kRankThreads) {
+      const uint32_t r0 = (uint32_t)__ldcs(in + i) - lo;
+      const uint32_t rk = rank_in(s, r0);
+      if (rk < kStage)
+        s.stage[rk] = r0;
+      else
+        __stcs(dst + rk, (int32_t)(r0 + lo));
+    }
+    __syncthreads();
+    // 4. staged ranks out in coalesced stores; clear the groups that were set
+    const uint32_t ns = size < kStage ? size : kStage;
+    for (uint32_t k = tid; k < ns; k += kRankThreads) __stcs(dst + k, (int32_t)(s.stage[k] + lo));
+#pragma unroll
+    for (uint32_t k = 0; k < kGroupsPer; ++k)
+      if (c[k]) bm4[tid * kGroupsPer + k] = make_uint4(0, 0, 0, 0);
     __syncthreads();
   }
 }
@@ -434,7 +485,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   const uint32_t G = 1u << (idbits - wbits);
   const uint32_t sms = (uint32_t)num_sms();
   const size_t small_bytes = sizeof(BucketSmem);
-  const size_t rank_bytes = sizeof(uint32_t) * (kBmWords + kSumWords);
+  const size_t rank_bytes = sizeof(RankSmem);
   const uint32_t nsets = (G <= kPerWarpMaxG) ? kTileWarps : 1u;
   const size_t scatter_bytes = (size_t)G * (8 + 4 + 4 * nsets) + kTile * 4;
   const size_t scatter_max = (size_t)(1u << (31 - kWinBits)) * 16 + kTile * 4;
@@ -510,8 +561,9 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
                                                                             wcur);
     mark(ws, kEvSortPart, s);
     ws->sort_part_marked = ws->timing;
-    const uint32_t grid = (uint32_t)(nw < (uint64_t)sms * 3 ? nw : (uint64_t)sms * 3);
-    k_win_sort<<<grid, kRankThreads, rank_bytes, s>>>(nw, G, wbits, whist, wbase, ws->tmp_ids, ws->out_ids);
+    const uint32_t grid = (uint32_t)(nw < (uint64_t)sms * 2 ? nw : (uint64_t)sms * 2);
+    k_win_sort<<<grid, kRankThreads, rank_bytes, s>>>((uint32_t)nw, G, wbits, whist, wbase, ws->tmp_ids,
+                                                      ws->out_ids);
     note_launch(5);
     st = check_launch("segmented sort windows");
     // the tables go back to the pool below: make sure the kernels are done
