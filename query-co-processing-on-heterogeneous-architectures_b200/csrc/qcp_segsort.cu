@@ -13,7 +13,7 @@
 //                           each bucket (a few ids) is insertion-sorted and
 //                           the order leaves in coalesced stores.
 //   larger slices           1. window partition: ids are split by
-//                              id >> wbits (wbits = min(idbits, 19)) into
+//                              id >> wbits (wbits = min(idbits, 18)) into
 //                              G = 2^(idbits - wbits) windows: tile
 //                              histograms -> per-slice window bases -> every
 //                              tile regrouped by window in shared memory and
@@ -21,11 +21,10 @@
 //                              buffer;
 //                           2. each (slice, window) is ranked through a
 //                              bitmap of its 2^wbits possible ids: every id
-//                              sets its bit, an exclusive popcount prefix
-//                              over groups of bitmap words gives each id its
-//                              rank, ids are placed at their rank in shared
-//                              memory and leave in coalesced stores -- no
-//                              comparisons, no divergence.
+//                              sets its bit, a prefix count over the words
+//                              follows, and every id goes to its rank
+//                              (bits before its word + bits below it in its
+//                              word) -- no comparisons.
 #include "qcp_internal.cuh"
 
 namespace qcp {
@@ -39,7 +38,7 @@ constexpr uint32_t kSmallWarps = kSmallThreads / 32;
 constexpr uint32_t kBucketBits = 11;
 constexpr uint32_t kBuckets = 1u << kBucketBits;
 // ---- window partition ------------------------------------------------------
-constexpr uint32_t kWinBits = 19;
+constexpr uint32_t kWinBits = 18;
 constexpr uint32_t kTile = 4096;
 constexpr uint32_t kTileThreads = 256;
 constexpr uint32_t kTileWarps = kTileThreads / 32;
@@ -47,7 +46,9 @@ constexpr uint32_t kPerWarpMaxG = 256;  // per-warp window counters up to this G
 // ---- window sort ------------------------------------------------------------
 constexpr uint32_t kRankThreads = 512;
 constexpr uint32_t kRankWarps = kRankThreads / 32;
-constexpr uint32_t kBmWords = (1u << kWinBits) / 32;  // 16384
+constexpr uint32_t kBmWords = (1u << kWinBits) / 32;  // 8192
+constexpr uint32_t kWarpWords = kBmWords / kRankWarps; // 512 words = 16384 ids: u16 prefixes
+constexpr uint32_t kStage = 6144;                      // staged output ids per window
 
 struct Job {
   unsigned long long off;
@@ -340,39 +341,25 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
 // ============================================================================
 // Window sort
 // ============================================================================
-constexpr uint32_t kGroups = kBmWords / 4;             // 4096 groups of 4 words
-constexpr uint32_t kGroupsPer = kGroups / kRankThreads; // 8 per thread
-constexpr uint32_t kStage = 8192;                      // ranked ids staged in smem
-
 struct RankSmem {
-  uint32_t bm[kBmWords];     // one bit per possible id of the window
-  uint32_t pre[kGroups];     // ids before each group of 4 words
-  uint32_t stage[kStage];    // ranks [0, kStage) on their way out
-  uint32_t wtot[kRankWarps];
+  uint32_t bm[kBmWords];        // one bit per possible id of the window
+  uint16_t pre[kBmWords];       // set bits before each word, within its warp's word range
+  int32_t stage[kStage];        // output positions [0, kStage) of the window
+  uint32_t wbase[kRankWarps];   // set bits before each warp's word range
 };
 
-// Rank of id offset r among the window's ids: the ids before r's group plus
-// the set bits below r inside the group (branch-free).
-__device__ __forceinline__ uint32_t rank_in(const RankSmem& s, uint32_t r) {
-  const uint32_t w = r >> 5;
-  const uint32_t sub = w & 3u;
-  const uint4 q = reinterpret_cast<const uint4*>(s.bm)[w >> 2];
-  const uint32_t below = (1u << (r & 31u)) - 1u;
-  const uint32_t m0 = sub > 0 ? 0xffffffffu : below;
-  const uint32_t m1 = sub > 1 ? 0xffffffffu : (sub == 1 ? below : 0u);
-  const uint32_t m2 = sub > 2 ? 0xffffffffu : (sub == 2 ? below : 0u);
-  const uint32_t m3 = sub == 3 ? below : 0u;
-  return s.pre[w >> 2] + __popc(q.x & m0) + __popc(q.y & m1) + __popc(q.z & m2) + __popc(q.w & m3);
-}
-
-// Persistent CTAs over the (job, window) pairs g = job * G + window: the ids
-// of window g (from src, the scratch buffer) are ranked through a bitmap of
-// the window's 2^wbits possible ids -- every id sets its bit, an exclusive
-// popcount prefix over groups of 4 bitmap words gives each id its rank --
-// placed at their rank in shared memory and written out in coalesced stores.
-// No comparisons, no divergence; the groups that were set are cleared from
-// the prefix pass's counts.
-__global__ void __launch_bounds__(kRankThreads, 2) k_win_sort(uint32_t total, uint32_t G, uint32_t wbits,
+// Persistent CTAs over the (job, window) pairs g = job * G + window.
+//   1. every id of window g (read from src, the scratch buffer) sets its bit
+//      in a bitmap of the window's 2^wbits possible ids;
+//   2. one sequential pass over the bitmap stores, per 32-bit word, the
+//      number of set bits before it (per warp range, plus warp bases);
+//   3. every id is read again (from L2) and goes to its rank
+//      = bits before its word + popc of its word below its bit;
+//      ranks below kStage are staged in shared memory and leave in
+//      coalesced stores, larger ranks are stored directly.
+// The ids of a window are distinct, so the ranks are a permutation of
+// [0, size) and the window comes out in ascending order.
+__global__ void __launch_bounds__(kRankThreads, 3) k_win_sort(uint32_t total, uint32_t G, uint32_t wbits,
                                                               const uint32_t* __restrict__ whist,
                                                               const unsigned long long* __restrict__ wbase,
                                                               const int32_t* __restrict__ src,
@@ -381,7 +368,10 @@ __global__ void __launch_bounds__(kRankThreads, 2) k_win_sort(uint32_t total, ui
   RankSmem& s = *reinterpret_cast<RankSmem*>(smem_raw);
   const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   uint4* bm4 = reinterpret_cast<uint4*>(s.bm);
-  for (uint32_t i = tid; i < kGroups; i += kRankThreads) bm4[i] = make_uint4(0, 0, 0, 0);
+  const uint32_t nwords = (1u << wbits) >> 5;   // wbits >= 5: slices here hold > 8192 ids
+  const uint32_t ngroups = nwords >> 2;         // groups of 4 words
+  const uint32_t w0 = wp * kWarpWords;          // this warp's word range [w0, w0 + kWarpWords)
+  for (uint32_t i = tid; i < kBmWords / 4; i += kRankThreads) bm4[i] = make_uint4(0, 0, 0, 0);
   __syncthreads();
   for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
     const uint32_t size = whist[g];
@@ -394,79 +384,84 @@ __global__ void __launch_bounds__(kRankThreads, 2) k_win_sort(uint32_t total, ui
       if (tid == 0) dst[0] = in[0];
       continue;
     }
-    // 1. set one bit per id
+    // 1. set one bit per id (the ids stay in L2 for step 3)
     uint32_t i = tid;
-    for (; i + 3 * kRankThreads < size; i += 4 * kRankThreads) {
-      const uint32_t a = (uint32_t)__ldcg(in + i) - lo, b = (uint32_t)__ldcg(in + i + kRankThreads) - lo;
-      const uint32_t c = (uint32_t)__ldcg(in + i + 2 * kRankThreads) - lo;
-      const uint32_t d = (uint32_t)__ldcg(in + i + 3 * kRankThreads) - lo;
-      atomicOr(&s.bm[a >> 5], 1u << (a & 31));
-      atomicOr(&s.bm[b >> 5], 1u << (b & 31));
-      atomicOr(&s.bm[c >> 5], 1u << (c & 31));
-      atomicOr(&s.bm[d >> 5], 1u << (d & 31));
+    for (; i + 7 * kRankThreads < size; i += 8 * kRankThreads) {
+      uint32_t a[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) a[k] = (uint32_t)in[i + k * kRankThreads] - lo;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) atomicOr(&s.bm[a[k] >> 5], 1u << (a[k] & 31));
     }
     for (; i < size; i += kRankThreads) {
-      const uint32_t a = (uint32_t)__ldcg(in + i) - lo;
+      const uint32_t a = (uint32_t)in[i] - lo;
       atomicOr(&s.bm[a >> 5], 1u << (a & 31));
     }
     __syncthreads();
-    // 2. exclusive popcount prefix over groups (kGroupsPer consecutive per thread)
-    uint32_t c[kGroupsPer];
-    uint32_t t = 0;
+    // 2. bits before every word, per warp range
+    uint32_t run = 0;
+    if (w0 < nwords) {
+      for (uint32_t gb = (w0 >> 2); gb < (w0 >> 2) + kWarpWords / 4; gb += 32) {
+        const uint32_t gi = gb + lane;
+        const uint4 q = (gi < ngroups) ? bm4[gi] : make_uint4(0, 0, 0, 0);
+        const uint32_t c0 = __popc(q.x), c1 = __popc(q.y), c2 = __popc(q.z), c3 = __popc(q.w);
+        const uint32_t t = c0 + c1 + c2 + c3;
+        uint32_t x = t;
 #pragma unroll
-    for (uint32_t k = 0; k < kGroupsPer; ++k) {
-      const uint4 q = bm4[tid * kGroupsPer + k];
-      c[k] = __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
-      t += c[k];
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= (uint32_t)o) x += y;
+        }
+        const uint32_t e = run + x - t;
+        if (gi < ngroups) {
+          uint2 pk;
+          pk.x = (e & 0xffffu) | ((e + c0) << 16);
+          pk.y = ((e + c0 + c1) & 0xffffu) | ((e + c0 + c1 + c2) << 16);
+          *reinterpret_cast<uint2*>(&s.pre[gi * 4]) = pk;
+        }
+        run += __shfl_sync(0xffffffffu, x, 31);
+      }
     }
-    uint32_t x = t;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= (uint32_t)o) x += y;
-    }
-    if (lane == 31) s.wtot[wp] = x;
+    if (lane == 0) s.wbase[wp] = run;
     __syncthreads();
-    uint32_t run = x - t;
-    for (uint32_t k = 0; k < wp; ++k) run += s.wtot[k];
+    if (wp == 0) {
+      const uint32_t v = lane < kRankWarps ? s.wbase[lane] : 0u;
+      uint32_t x = v;
 #pragma unroll
-    for (uint32_t k = 0; k < kGroupsPer; ++k) {
-      s.pre[tid * kGroupsPer + k] = run;
-      run += c[k];
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+      }
+      __syncwarp();
+      if (lane < kRankWarps) s.wbase[lane] = x - v;
     }
     __syncthreads();
-    // 3. rank every id (read again, from L2); ranks past kStage go straight out
+    // 3. every id to its rank
     i = tid;
     for (; i + 3 * kRankThreads < size; i += 4 * kRankThreads) {
-      uint32_t r[4];
-      r[0] = (uint32_t)__ldcs(in + i) - lo;
-      r[1] = (uint32_t)__ldcs(in + i + kRankThreads) - lo;
-      r[2] = (uint32_t)__ldcs(in + i + 2 * kRankThreads) - lo;
-      r[3] = (uint32_t)__ldcs(in + i + 3 * kRankThreads) - lo;
+      uint32_t a[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a[k] = (uint32_t)__ldcs(in + i + k * kRankThreads) - lo;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        const uint32_t rk = rank_in(s, r[k]);
-        if (rk < kStage)
-          s.stage[rk] = r[k];
-        else
-          __stcs(dst + rk, (int32_t)(r[k] + lo));
+        const uint32_t wd = a[k] >> 5;
+        const uint32_t r = s.wbase[wd / kWarpWords] + s.pre[wd] + __popc(s.bm[wd] & ((1u << (a[k] & 31)) - 1u));
+        if (r < kStage) s.stage[r] = (int32_t)(a[k] + lo);
+        else dst[r] = (int32_t)(a[k] + lo);
       }
     }
     for (; i < size; i += kRankThreads) {
-      const uint32_t r0 = (uint32_t)__ldcs(in + i) - lo;
-      const uint32_t rk = rank_in(s, r0);
-      if (rk < kStage)
-        s.stage[rk] = r0;
-      else
-        __stcs(dst + rk, (int32_t)(r0 + lo));
+      const uint32_t a = (uint32_t)__ldcs(in + i) - lo;
+      const uint32_t wd = a >> 5;
+      const uint32_t r = s.wbase[wd / kWarpWords] + s.pre[wd] + __popc(s.bm[wd] & ((1u << (a & 31)) - 1u));
+      if (r < kStage) s.stage[r] = (int32_t)(a + lo);
+      else dst[r] = (int32_t)(a + lo);
     }
     __syncthreads();
-    // 4. staged ranks out in coalesced stores; clear the groups that were set
+    // 4. staged ranks out, bitmap cleared
     const uint32_t ns = size < kStage ? size : kStage;
-    for (uint32_t k = tid; k < ns; k += kRankThreads) __stcs(dst + k, (int32_t)(s.stage[k] + lo));
-#pragma unroll
-    for (uint32_t k = 0; k < kGroupsPer; ++k)
-      if (c[k]) bm4[tid * kGroupsPer + k] = make_uint4(0, 0, 0, 0);
+    for (uint32_t k = tid; k < ns; k += kRankThreads) dst[k] = s.stage[k];
+    for (uint32_t k = tid; k < ngroups; k += kRankThreads) bm4[k] = make_uint4(0, 0, 0, 0);
     __syncthreads();
   }
 }
@@ -561,7 +556,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
                                                                             wcur);
     mark(ws, kEvSortPart, s);
     ws->sort_part_marked = ws->timing;
-    const uint32_t grid = (uint32_t)(nw < (uint64_t)sms * 2 ? nw : (uint64_t)sms * 2);
+    const uint32_t grid = (uint32_t)(nw < (uint64_t)sms * 3 ? nw : (uint64_t)sms * 3);
     k_win_sort<<<grid, kRankThreads, rank_bytes, s>>>((uint32_t)nw, G, wbits, whist, wbase, ws->tmp_ids,
                                                       ws->out_ids);
     note_launch(5);
