@@ -116,16 +116,26 @@ def dist_setup(n_gpus):
 
 
 def algorithmic_bytes(st: dict, dims: int, fanout: int) -> dict:
-    """Bytes each phase must move at minimum for the work it did:
-    count  leaf-MBR reads of every (query, leaf-parent) item + coordinates of
-           partially covered leaves
-    write  the same reads again + 4 B id read and 4 B id write per hit
-    sort   small slices 8 B/hit (one read, one write), MSD slices 20 B/hit
+    """Bytes each kernel must move at minimum for the work it did, per launch
+    (one launch of each per step):
+    k_leafscan<count>  leaf-MBR reads of every (query, leaf-parent) item +
+                       coordinates of partially covered leaves
+    k_leafscan<write>  the same reads again + 4 B id read and 4 B id write per hit
+    k_sort_small       4 B read + 4 B write per id of the slices <= 8192 ids
+    k_win_sort         4 B read + 4 B write per id of the larger slices
     """
     mbr = st["leaf_items"] * fanout * 2 * dims * 4
     coords = st["leaves_partial"] * fanout * dims * 4
     hits = st["hits"]
-    return {"count": mbr + coords, "write": mbr + coords + 8 * hits, "sort": 8 * hits}
+    win = st["sort_window_ids"]
+    return {"count": mbr + coords, "write": mbr + coords + 8 * hits,
+            "sort_small": 8 * (hits - win), "sort_windows": 8 * win}
+
+
+# DRAM bytes (read + write) per id of k_win_sort from an ncu capture of the
+# 16M-point Gaussian workload at 2,000 queries (profiles/k_win_sort_gauss16m_q2000.md),
+# applied to the ids of the timed launch: traffic grows with the ids processed.
+K_WIN_SORT_DRAM_BYTES_PER_ID = (851630848 + 797769216) / 211501325  # 7.80 B per id
 
 
 def run_ours(args, rank, world, local):
@@ -216,13 +226,20 @@ def run_ours(args, rank, world, local):
     value = world * Q * args.steps / (elapsed_ms / 1e3)
 
     # ---- roofline of the dominant kernel ------------------------------------
+    # every candidate is ONE kernel launched once per step, timed by the
+    # library's CUDA events on the launching stream
     hbm, peak_kind = peaks()
-    dominant = max(["count", "write", "sort"], key=lambda k: phase[k])
-    ab = algorithmic_bytes(stats, w.dims, args.fanout)
     kernel_names = {"count": "k_leafscan<count>", "write": "k_leafscan<write>",
-                    "sort": "segmented sort (k_sort_small + MSD kernels)"}
+                    "sort_small": "k_sort_small", "sort_windows": "k_win_sort"}
+    ab = algorithmic_bytes(stats, w.dims, args.fanout)
+    dominant = max(kernel_names, key=lambda k: phase[k])
     per_launch_ms = phase[dominant] / args.steps
     achieved = ab[dominant] / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
+    traffic = None
+    if dominant == "sort_windows" and K_WIN_SORT_DRAM_BYTES_PER_ID:
+        traffic = int(K_WIN_SORT_DRAM_BYTES_PER_ID * stats["sort_window_ids"])
+    kernels_gbs = {kernel_names[k]: round(ab[k] / (phase[k] / args.steps / 1e3) / 1e9, 1)
+                   for k in kernel_names if phase[k] > 0}
 
     # ---- plain one-query-per-block traversal, same batch -------------------
     plain = None
@@ -306,12 +323,14 @@ def run_ours(args, rank, world, local):
         "build_ms": round(build_ms, 2),
         "phase_ms_per_step": {k: round(v / args.steps, 4) for k, v in phase.items()},
         "work_per_step": {k: stats[k] for k in ["leaf_items", "leaves_covered", "leaves_partial",
-                                                 "objects_covered", "sort_small_jobs", "sort_msd_jobs"]},
+                                                 "objects_covered", "sort_small_jobs", "sort_msd_jobs",
+                                                 "sort_window_ids"]},
         "roofline": {"bound": "hbm", "kernel": kernel_names[dominant],
                      "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                     "frac": round(achieved / hbm, 4), "traffic": None,
-                     "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": int(ab[dominant])},
+                     "frac": round(achieved / hbm, 4), "traffic": traffic,
+                     "peak_kind": peak_kind, "launch_ms": round(per_launch_ms, 4),
+                     "algorithmic_bytes_per_launch": int(ab[dominant]),
+                     "kernels_achieved_gbs": kernels_gbs},
         "plain": {"value": round(plain, 1) if plain else None, "unit": "queries/s",
                   "speedup_batched_vs_plain": round(value / plain, 2) if plain else None},
         "e2e": {"value": round(e2e_value, 1), "unit": "queries/s", "h2d_bytes_per_step": int(h2d),

@@ -128,6 +128,7 @@ typedef struct qcp_query_stats {
   float ms_expand, ms_count, ms_scan, ms_write, ms_sort, ms_total;
   /* parts of ms_sort: small slices, window partition, window sort */
   float ms_sort_small, ms_sort_partition, ms_sort_windows;
+  uint64_t sort_window_ids;    /* ids of the slices sorted through windows (with QCP_QUERY_TIMING) */
 } qcp_query_stats;
 
 qcp_status qcp_query_stats_last(qcp_query_stats* out);

@@ -71,7 +71,7 @@ class QueryStats(ctypes.Structure):
                 ("ms_scan", ctypes.c_float), ("ms_write", ctypes.c_float),
                 ("ms_sort", ctypes.c_float), ("ms_total", ctypes.c_float),
                 ("ms_sort_small", ctypes.c_float), ("ms_sort_partition", ctypes.c_float),
-                ("ms_sort_windows", ctypes.c_float)]
+                ("ms_sort_windows", ctypes.c_float), ("sort_window_ids", ctypes.c_uint64)]
 
 
 class Result(ctypes.Structure):

@@ -576,6 +576,7 @@ static qcp_status run_query(qcp_index* ix, const float* boxes, uint32_t q, const
       t_stats.leaves_covered = ws->h_stats[kStatCovered];
       t_stats.leaves_partial = ws->h_stats[kStatPartial];
       t_stats.objects_covered = ws->h_stats[kStatObjCovered];
+      t_stats.sort_window_ids = ws->h_stats[kStatWindowIds];
       for (int l = 0; l < 16; ++l) t_stats.frontier_items[l] = ws->h_stats[kStatLevel0 + l];
       t_stats.leaf_items = t_stats.frontier_items[1];
       auto ms = [&](int a, int b) {

@@ -114,6 +114,7 @@ enum StatSlot : uint32_t {
   kStatCovered = 0,     // covered leaves
   kStatPartial = 1,     // partially covered leaves (objects tested)
   kStatObjCovered = 2,  // objects in covered leaves
+  kStatWindowIds = 3,   // ids of the slices sorted through windows
   kStatLevel0 = 8,      // frontier items of level l at kStatLevel0 + l
   kStatCount = 24
 };

@@ -49,6 +49,8 @@ constexpr uint32_t kRankWarps = kRankThreads / 32;
 constexpr uint32_t kBmWords = (1u << kWinBits) / 32;  // 8192
 constexpr uint32_t kWarpWords = kBmWords / kRankWarps; // 512 words = 16384 ids: u16 prefixes
 constexpr uint32_t kStage = 6144;                      // staged output ids per window
+constexpr uint32_t kBatch = 8;                         // ids per thread per load round
+constexpr uint32_t kNone = 0xffffffffu;                // empty register slot
 
 struct Job {
   unsigned long long off;
@@ -159,7 +161,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_sort_small(const Job* __restr
 // Window partition
 // ============================================================================
 __global__ void k_classify(const unsigned long long* __restrict__ offsets, uint32_t q, Job* small,
-                           uint32_t* nsmall, Job* big, uint32_t* nbig) {
+                           uint32_t* nsmall, Job* big, uint32_t* nbig, unsigned long long* big_ids) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < q; i += gridDim.x * blockDim.x) {
     const unsigned long long off = offsets[i];
     const unsigned long long sz = offsets[i + 1] - off;
@@ -172,6 +174,7 @@ __global__ void k_classify(const unsigned long long* __restrict__ offsets, uint3
       small[atomicAdd(nsmall, 1u)] = j;
     } else {
       big[atomicAdd(nbig, 1u)] = j;
+      if (big_ids) atomicAdd(big_ids, sz);
     }
   }
 }
@@ -384,18 +387,19 @@ __global__ void __launch_bounds__(kRankThreads, 3) k_win_sort(uint32_t total, ui
       if (tid == 0) dst[0] = in[0];
       continue;
     }
-    // 1. set one bit per id (the ids stay in L2 for step 3)
-    uint32_t i = tid;
-    for (; i + 7 * kRankThreads < size; i += 8 * kRankThreads) {
-      uint32_t a[8];
+    // 1. set one bit per id (the ids stay in L2 for step 3).  All loads of a
+    //    round are issued before the first atomic: one memory latency per
+    //    4096 ids instead of one per id of the thread.
+    for (uint32_t i0 = 0; i0 < size; i0 += kBatch * kRankThreads) {
+      uint32_t a[kBatch];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) a[k] = (uint32_t)in[i + k * kRankThreads] - lo;
+      for (uint32_t k = 0; k < kBatch; ++k) {
+        const uint32_t i = i0 + k * kRankThreads + tid;
+        a[k] = i < size ? (uint32_t)in[i] - lo : kNone;
+      }
 #pragma unroll
-      for (int k = 0; k < 8; ++k) atomicOr(&s.bm[a[k] >> 5], 1u << (a[k] & 31));
-    }
-    for (; i < size; i += kRankThreads) {
-      const uint32_t a = (uint32_t)in[i] - lo;
-      atomicOr(&s.bm[a >> 5], 1u << (a & 31));
+      for (uint32_t k = 0; k < kBatch; ++k)
+        if (a[k] != kNone) atomicOr(&s.bm[a[k] >> 5], 1u << (a[k] & 31));
     }
     __syncthreads();
     // 2. bits before every word, per warp range
@@ -437,25 +441,21 @@ __global__ void __launch_bounds__(kRankThreads, 3) k_win_sort(uint32_t total, ui
     }
     __syncthreads();
     // 3. every id to its rank
-    i = tid;
-    for (; i + 3 * kRankThreads < size; i += 4 * kRankThreads) {
-      uint32_t a[4];
+    for (uint32_t i0 = 0; i0 < size; i0 += kBatch * kRankThreads) {
+      uint32_t a[kBatch];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) a[k] = (uint32_t)__ldcs(in + i + k * kRankThreads) - lo;
+      for (uint32_t k = 0; k < kBatch; ++k) {
+        const uint32_t i = i0 + k * kRankThreads + tid;
+        a[k] = i < size ? (uint32_t)__ldcs(in + i) - lo : kNone;
+      }
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
+      for (uint32_t k = 0; k < kBatch; ++k) {
+        if (a[k] == kNone) continue;
         const uint32_t wd = a[k] >> 5;
         const uint32_t r = s.wbase[wd / kWarpWords] + s.pre[wd] + __popc(s.bm[wd] & ((1u << (a[k] & 31)) - 1u));
         if (r < kStage) s.stage[r] = (int32_t)(a[k] + lo);
         else dst[r] = (int32_t)(a[k] + lo);
       }
-    }
-    for (; i < size; i += kRankThreads) {
-      const uint32_t a = (uint32_t)__ldcs(in + i) - lo;
-      const uint32_t wd = a >> 5;
-      const uint32_t r = s.wbase[wd / kWarpWords] + s.pre[wd] + __popc(s.bm[wd] & ((1u << (a & 31)) - 1u));
-      if (r < kStage) s.stage[r] = (int32_t)(a + lo);
-      else dst[r] = (int32_t)(a + lo);
     }
     __syncthreads();
     // 4. staged ranks out, bitmap cleared
@@ -499,7 +499,8 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   Job* small = reinterpret_cast<Job*>(ws->jobs[0]);
   Job* big = reinterpret_cast<Job*>(ws->jobs[1]);
   k_classify<<<(q + 255) / 256, 256, 0, s>>>((const unsigned long long*)ws->offsets, q, small,
-                                             ctr + kCtrJobs0, big, ctr + kCtrJobs1);
+                                             ctr + kCtrJobs0, big, ctr + kCtrJobs1,
+                                             ws->timing ? ws->d_stats + kStatWindowIds : nullptr);
   note_launch();
   QCP_CUDA(cudaMemcpyAsync(ws->h_ctr, ctr, sizeof(uint32_t) * kCtrCount, cudaMemcpyDeviceToHost, s));
   QCP_CUDA(cudaStreamSynchronize(s));
