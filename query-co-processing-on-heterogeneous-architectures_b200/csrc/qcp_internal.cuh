@@ -230,6 +230,17 @@ __host__ __device__ inline uint64_t hilbert_index(uint32_t dims, uint32_t bits, 
   return index & low_ones64(total);
 }
 
+// One per-query slice handed to the sort kernels: output offset, size and
+// query index.
+struct SortJob {
+  unsigned long long off;
+  uint32_t size;
+  uint32_t q;
+};
+
+// Slices of at most this many ids are sorted whole in shared memory.
+constexpr uint32_t kSmallSliceCap = 8192;
+
 // ---------------------------------------------------------------------------
 // Kernel launchers (defined in the .cu files)
 // ---------------------------------------------------------------------------
@@ -251,7 +262,19 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
                        cudaStream_t s);
 qcp_status run_plain(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_only, bool sort,
                      cudaStream_t s);
+// Steps of the batched pipeline (qcp_search.cu): root items of every query
+// into items[0]; (query, node) items of level l in items[cur] -> items of
+// level l - 1 in items[cur ^ 1]; unsorted write of the level-1 items in
+// items[cur] whose item_hits are nonzero.
+qcp_status init_items(Workspace* ws, uint32_t q, cudaStream_t s);
+qcp_status expand_level(qcp_index* ix, Workspace* ws, uint32_t l, int cur, cudaStream_t s);
+qcp_status write_items(qcp_index* ix, Workspace* ws, int cur, cudaStream_t s);
 qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t s);
+// Sorts the slices of <= kSmallSliceCap ids; the larger slices are returned
+// as a device job list (big, *nbig entries) for the caller.
+qcp_status sort_small_slices(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t s,
+                             const SortJob** big, uint32_t* nbig);
+
 qcp_status run_batched_counts_into(qcp_index* ix, const float* boxes, uint32_t q, uint64_t* counts,
                                    uint2* items0, uint2* items1, uint32_t* item_hits, size_t item_cap,
                                    uint32_t* ctr, unsigned long long* stats, cudaStream_t s);

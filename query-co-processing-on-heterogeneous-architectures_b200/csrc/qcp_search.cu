@@ -26,107 +26,11 @@
 #include <cfloat>
 
 #include "qcp_internal.cuh"
+#include "qcp_tree.cuh"
 
 namespace qcp {
 
 namespace {
-
-struct TreeView {
-  const float* coords;
-  const int32_t* ids;
-  uint64_t n, npad;
-  uint32_t fanout, levels;
-  const float* mbr[kMaxLevels];
-  uint64_t nodes[kMaxLevels];
-  uint64_t pad[kMaxLevels];
-};
-
-TreeView view_of(const qcp_index* ix) {
-  TreeView v;
-  v.coords = ix->coords;
-  v.ids = ix->ids;
-  v.n = ix->n;
-  v.npad = ix->npad;
-  v.fanout = ix->fanout;
-  v.levels = ix->levels;
-  for (int l = 0; l < kMaxLevels; ++l) {
-    v.mbr[l] = ix->mbr[l];
-    v.nodes[l] = ix->level_nodes[l];
-    v.pad[l] = ix->level_pad[l];
-  }
-  return v;
-}
-
-template <int D>
-struct Box {
-  float lo[D], hi[D];
-};
-
-template <int D>
-__device__ __forceinline__ Box<D> load_box(const float* boxes, uint32_t q) {
-  Box<D> b;
-  const float* p = boxes + (uint64_t)q * 2 * D;
-#pragma unroll
-  for (int d = 0; d < D; ++d) {
-    b.lo[d] = __ldg(p + d);
-    b.hi[d] = __ldg(p + D + d);
-  }
-  return b;
-}
-
-// MBR overlap / containment of node c of a level.
-template <int D>
-__device__ __forceinline__ void test_node(const Box<D>& b, const float* mbr, uint64_t pad, uint64_t c,
-                                          bool& ov, bool& in) {
-  ov = true;
-  in = true;
-#pragma unroll
-  for (int d = 0; d < D; ++d) {
-    const float lo = __ldg(mbr + (uint64_t)d * pad + c);
-    const float hi = __ldg(mbr + (uint64_t)(D + d) * pad + c);
-    ov &= overlaps1(b.lo[d], b.hi[d], lo, hi);
-    in &= inside1(b.lo[d], b.hi[d], lo, hi);
-  }
-}
-
-// Hit mask of 4 consecutive objects starting at position p (p % 4 == 0).
-template <int D, bool RECT>
-__device__ __forceinline__ uint32_t test4(const Box<D>& b, const float* coords, uint64_t npad, uint64_t p,
-                                          uint64_t n) {
-  uint32_t m = 0xfu;
-#pragma unroll
-  for (int d = 0; d < D; ++d) {
-    const float4 lo = __ldg(reinterpret_cast<const float4*>(coords + (uint64_t)d * npad + p));
-    float4 hi = lo;
-    if (RECT) hi = __ldg(reinterpret_cast<const float4*>(coords + (uint64_t)(D + d) * npad + p));
-    m &= (overlaps1(b.lo[d], b.hi[d], lo.x, hi.x) ? 1u : 0u) | (overlaps1(b.lo[d], b.hi[d], lo.y, hi.y) ? 2u : 0u) |
-         (overlaps1(b.lo[d], b.hi[d], lo.z, hi.z) ? 4u : 0u) | (overlaps1(b.lo[d], b.hi[d], lo.w, hi.w) ? 8u : 0u);
-  }
-  // objects past n (padding of the last leaf) never hit
-  if (p + 4 > n) {
-    const uint64_t valid = (n > p) ? (n - p) : 0;
-    m &= (1u << valid) - 1u;
-  }
-  return m;
-}
-
-__device__ __forceinline__ uint32_t lane_lt_mask() {
-  uint32_t m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
-
-__device__ __forceinline__ uint32_t warp_excl_sum(uint32_t v, uint32_t* total) {
-  const uint32_t lane = threadIdx.x & 31;
-  uint32_t x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= (uint32_t)o) x += y;
-  }
-  *total = __shfl_sync(0xffffffffu, x, 31);
-  return x - v;
-}
 
 // ---------------------------------------------------------------------------
 // Batched pipeline kernels
@@ -412,19 +316,6 @@ __global__ void __launch_bounds__(256) k_mprs(TreeView t, const float* __restric
   }
 }
 
-#define QCP_DISPATCH_D(D_, ...)                  \
-  switch (D_) {                                  \
-    case 1: { constexpr int DD = 1; __VA_ARGS__; } break; \
-    case 2: { constexpr int DD = 2; __VA_ARGS__; } break; \
-    case 3: { constexpr int DD = 3; __VA_ARGS__; } break; \
-    case 4: { constexpr int DD = 4; __VA_ARGS__; } break; \
-    case 5: { constexpr int DD = 5; __VA_ARGS__; } break; \
-    case 6: { constexpr int DD = 6; __VA_ARGS__; } break; \
-    case 7: { constexpr int DD = 7; __VA_ARGS__; } break; \
-    case 8: { constexpr int DD = 8; __VA_ARGS__; } break; \
-    default: break;                              \
-  }
-
 template <int D>
 void launch_expand(uint32_t grid, cudaStream_t s, const float* boxes, const uint2* in,
                    const uint32_t* in_count, uint2* out, uint32_t* out_count, uint64_t cap,
@@ -470,6 +361,37 @@ qcp_status ws_reserve_queries(qcp_index* ix, Workspace* ws, uint32_t q);
 qcp_status ws_reserve_items(qcp_index* ix, Workspace* ws, size_t items);
 qcp_status ws_reserve_out(qcp_index* ix, Workspace* ws, size_t ids);
 
+qcp_status init_items(Workspace* ws, uint32_t q, cudaStream_t s) {
+  k_init_items<<<(q + 255) / 256, 256, 0, s>>>(ws->items[0], q, 0, ws->ctr + kCtrFrontier0);
+  note_launch();
+  return QCP_OK;
+}
+
+qcp_status expand_level(qcp_index* ix, Workspace* ws, uint32_t l, int cur, cudaStream_t s) {
+  const TreeView t = view_of(ix);
+  const uint32_t grid = (uint32_t)num_sms() * 8;  // 8 x 256 threads resident per SM
+  const int nxt = cur ^ 1;
+  uint32_t* ctr = ws->ctr;
+  QCP_DISPATCH_D(ix->dims, launch_expand<DD>(grid, s, ws->boxes, ws->items[cur], ctr + kCtrFrontier0 + cur,
+                                             ws->items[nxt], ctr + kCtrFrontier0 + nxt, ws->items_cap,
+                                             t.mbr[l - 1], t.nodes[l - 1], t.pad[l - 1], t.fanout,
+                                             ctr + kCtrOverflow, ctr + kCtrNeedItems));
+  note_launch();
+  return check_launch("k_expand");
+}
+
+qcp_status write_items(qcp_index* ix, Workspace* ws, int cur, cudaStream_t s) {
+  const TreeView t = view_of(ix);
+  const uint32_t grid = (uint32_t)num_sms() * 8;
+  uint32_t* ctr = ws->ctr;
+  QCP_DISPATCH_D(ix->dims, launch_leafscan<DD, kWrite>(ix->is_rect != 0, grid, s, t, ws->boxes, ws->items[cur],
+                                                       ctr + kCtrFrontier0 + cur, ctr + kCtrWork,
+                                                       ws->item_hits, nullptr, ws->offsets, ws->qcursor,
+                                                       ws->out_ids, ws->items_cap, ws->d_stats));
+  note_launch();
+  return check_launch("k_leafscan<write>");
+}
+
 qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_only, bool sort,
                        cudaStream_t s) {
   const TreeView t = view_of(ix);
@@ -485,24 +407,18 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
     QCP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * kCtrCount, s));
     QCP_CUDA(cudaMemsetAsync(ws->d_stats, 0, sizeof(unsigned long long) * kStatCount, s));
     QCP_CUDA(cudaMemsetAsync(ws->qcount, 0, sizeof(uint64_t) * q, s));
-    k_init_items<<<(q + 255) / 256, 256, 0, s>>>(ws->items[0], q, 0, ctr + kCtrFrontier0);
-    note_launch();
+    QCP_TRY(init_items(ws, q, s));
     QCP_CUDA(cudaMemcpyAsync(ws->d_stats + kStatLevel0 + start, ctr + kCtrFrontier0, sizeof(uint32_t),
                              cudaMemcpyDeviceToDevice, s));
     int cur = 0;
     for (uint32_t l = start; l > 1; --l) {
       const int nxt = cur ^ 1;
       QCP_CUDA(cudaMemsetAsync(ctr + kCtrFrontier0 + nxt, 0, sizeof(uint32_t), s));
-      QCP_DISPATCH_D(D, launch_expand<DD>(grid, s, ws->boxes, ws->items[cur], ctr + kCtrFrontier0 + cur,
-                                          ws->items[nxt], ctr + kCtrFrontier0 + nxt, ws->items_cap,
-                                          t.mbr[l - 1], t.nodes[l - 1], t.pad[l - 1], t.fanout,
-                                          ctr + kCtrOverflow, ctr + kCtrNeedItems));
-      note_launch();
+      QCP_TRY(expand_level(ix, ws, l, cur, s));
       QCP_CUDA(cudaMemcpyAsync(ws->d_stats + kStatLevel0 + (l - 1), ctr + kCtrFrontier0 + nxt,
                                sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
       cur = nxt;
     }
-    QCP_TRY(check_launch("k_expand"));
     mark(ws, kEvExpand, s);
     // the level-1 items must fit the per-item hit array too
     QCP_TRY(ws_reserve_items(ix, ws, 0));
@@ -531,12 +447,7 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
     if (total) {
       QCP_CUDA(cudaMemsetAsync(ws->qcursor, 0, sizeof(uint64_t) * q, s));
       QCP_CUDA(cudaMemsetAsync(ctr + kCtrWork, 0, sizeof(uint32_t), s));
-      QCP_DISPATCH_D(D, launch_leafscan<DD, kWrite>(rect, grid, s, t, ws->boxes, ws->items[cur],
-                                                    ctr + kCtrFrontier0 + cur, ctr + kCtrWork,
-                                                    ws->item_hits, nullptr, ws->offsets, ws->qcursor,
-                                                    ws->out_ids, ws->items_cap, ws->d_stats));
-      note_launch();
-      QCP_TRY(check_launch("k_leafscan<write>"));
+      QCP_TRY(write_items(ix, ws, cur, s));
       mark(ws, kEvWrite, s);
       if (sort) QCP_TRY(segmented_sort(ix, ws, q, s));
       mark(ws, kEvSort, s);

@@ -32,7 +32,7 @@ namespace qcp {
 namespace {
 
 // ---- small slices ----------------------------------------------------------
-constexpr uint32_t kSmallCap = 8192;
+constexpr uint32_t kSmallCap = kSmallSliceCap;
 constexpr uint32_t kSmallThreads = 256;
 constexpr uint32_t kSmallWarps = kSmallThreads / 32;
 constexpr uint32_t kBucketBits = 11;
@@ -52,11 +52,7 @@ constexpr uint32_t kStage = 6144;                      // staged output ids per 
 constexpr uint32_t kBatch = 8;                         // ids per thread per load round
 constexpr uint32_t kNone = 0xffffffffu;                // empty register slot
 
-struct Job {
-  unsigned long long off;
-  uint32_t size;
-  uint32_t pad;
-};
+using Job = SortJob;
 
 // ============================================================================
 // Small slices: bucket sort
@@ -169,7 +165,7 @@ __global__ void k_classify(const unsigned long long* __restrict__ offsets, uint3
     Job j;
     j.off = off;
     j.size = (uint32_t)sz;
-    j.pad = 0;
+    j.q = i;
     if (sz <= kSmallCap) {
       small[atomicAdd(nsmall, 1u)] = j;
     } else {
@@ -470,29 +466,36 @@ __global__ void __launch_bounds__(kRankThreads, 3) k_win_sort(uint32_t total, ui
 
 qcp_status ws_reserve_sort(qcp_index* ix, Workspace* ws, size_t jobs, size_t tiles);
 
-qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t s) {
-  ws->sort_small_jobs = ws->sort_msd_jobs = 0;
-  ws->sort_part_marked = false;
-  if (q == 0) return QCP_OK;
+static uint32_t id_bits(uint64_t n) {
   uint32_t idbits = 1;
-  while (idbits < 31 && (1ull << idbits) < ix->n) ++idbits;
-  const uint32_t wbits = idbits < kWinBits ? idbits : kWinBits;
-  const uint32_t G = 1u << (idbits - wbits);
-  const uint32_t sms = (uint32_t)num_sms();
-  const size_t small_bytes = sizeof(BucketSmem);
-  const size_t rank_bytes = sizeof(RankSmem);
-  const uint32_t nsets = (G <= kPerWarpMaxG) ? kTileWarps : 1u;
-  const size_t scatter_bytes = (size_t)G * (8 + 4 + 4 * nsets) + kTile * 4;
-  const size_t scatter_max = (size_t)(1u << (31 - kWinBits)) * 16 + kTile * 4;
+  while (idbits < 31 && (1ull << idbits) < n) ++idbits;
+  return idbits;
+}
+
+static qcp_status set_sort_attrs(const qcp_index* ix, size_t scatter_max) {
   static thread_local int attrs_device = -1;  // attributes are per device
   if (attrs_device != ix->device) {
-    QCP_CUDA(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_bytes));
-    QCP_CUDA(cudaFuncSetAttribute(k_win_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rank_bytes));
+    QCP_CUDA(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(BucketSmem)));
+    QCP_CUDA(cudaFuncSetAttribute(k_win_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(RankSmem)));
     QCP_CUDA(cudaFuncSetAttribute(k_win_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(scatter_max > scatter_bytes ? scatter_max : scatter_bytes)));
+                                  (int)scatter_max));
     attrs_device = ix->device;
   }
+  return QCP_OK;
+}
 
+qcp_status sort_small_slices(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t s,
+                             const SortJob** big_out, uint32_t* nbig_out) {
+  *big_out = nullptr;
+  *nbig_out = 0;
+  ws->sort_small_jobs = ws->sort_msd_jobs = 0;
+  if (q == 0) return QCP_OK;
+  const uint32_t idbits = id_bits(ix->n);
+  const uint32_t sms = (uint32_t)num_sms();
+  const size_t scatter_max = (size_t)(1u << (31 - kWinBits)) * 16 + kTile * 4;
+  QCP_TRY(set_sort_attrs(ix, scatter_max));
   QCP_TRY(ws_reserve_sort(ix, ws, (size_t)q + 256, 0));
   uint32_t* ctr = ws->ctr;
   QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t) * 2, s));
@@ -509,12 +512,32 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   ws->sort_small_jobs = nsmall;
   ws->sort_msd_jobs = nbig;
   if (nsmall) {
-    k_sort_small<<<min(nsmall, sms * 3), kSmallThreads, small_bytes, s>>>(small, nsmall, ws->out_ids, idbits);
+    k_sort_small<<<min(nsmall, sms * 3), kSmallThreads, sizeof(BucketSmem), s>>>(small, nsmall, ws->out_ids,
+                                                                                  idbits);
     note_launch();
     QCP_TRY(check_launch("k_sort_small"));
   }
+  *big_out = big;
+  *nbig_out = nbig;
+  return QCP_OK;
+}
+
+qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t s) {
+  ws->sort_part_marked = false;
+  const Job* bigc = nullptr;
+  uint32_t nbig = 0;
+  QCP_TRY(sort_small_slices(ix, ws, q, s, &bigc, &nbig));
   mark(ws, kEvSortSmall, s);
   if (nbig == 0) return QCP_OK;
+  Job* big = const_cast<Job*>(bigc);
+  uint32_t* ctr = ws->ctr;
+  const uint32_t idbits = id_bits(ix->n);
+  const uint32_t wbits = idbits < kWinBits ? idbits : kWinBits;
+  const uint32_t G = 1u << (idbits - wbits);
+  const uint32_t sms = (uint32_t)num_sms();
+  const size_t rank_bytes = sizeof(RankSmem);
+  const uint32_t nsets = (G <= kPerWarpMaxG) ? kTileWarps : 1u;
+  const size_t scatter_bytes = (size_t)G * (8 + 4 + 4 * nsets) + kTile * 4;
 
   // tables per (job, window): counts (u32), bases and cursors (u64); tiles
   // and tile offsets per job
