@@ -282,6 +282,27 @@ def run_ours(args, rank, world, local):
     e2e_ms = max_over_ranks(e_a.elapsed_time(e_b))
     e2e_value = world * Q * args.e2e_steps / (e2e_ms / 1e3)
 
+    # ---- serving: open-loop Poisson arrivals through continuous batching ----
+    serving = None
+    if args.serve_seconds > 0 and world == 1:
+        t_arr, s_boxes, s_cls = W.serving_stream(w.objs, rate=args.serve_rate, duration_s=args.serve_seconds)
+        # warm-up: a burst at t = 0 sizes every stream's workspace for full
+        # batches, then a short open-loop run
+        nburst = min(len(s_boxes), 4 * 16384 * args.serve_streams)
+        ix.serve(s_boxes[:nburst], np.zeros(nburst), streams=args.serve_streams, max_batch=16384)
+        ix.serve(s_boxes[:20000], t_arr[:20000] - t_arr[0], streams=args.serve_streams)
+        st, lat, _ = ix.serve(s_boxes, t_arr, streams=args.serve_streams, max_batch=16384,
+                              output_cap_bytes=2 << 30)
+        serving = {"workload": "config-2 index; Poisson %.0f req/s for %.1f s; cube volumes 1e-7/1e-5/1e-3 "
+                               "at 70/25/5%%" % (args.serve_rate, args.serve_seconds),
+                   "requests": int(st["requests"]), "sustained_qps": round(st["qps"], 1),
+                   "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+                   "max_ms": round(st["max_ms"], 3), "mean_batch": round(st["mean_batch"], 1),
+                   "batches": int(st["batches"]), "max_inflight": int(st["max_inflight"]),
+                   "hits_per_request": round(st["hits"] / max(1, st["requests"]), 1),
+                   "output_cap_bytes": 2 << 30, "max_output_bytes": int(st["max_output_bytes"]),
+                   "streams": args.serve_streams}
+
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -338,6 +359,8 @@ def run_ours(args, rank, world, local):
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    if serving is not None:
+        out["serving"] = serving
     if cpu is not None:
         out["cpu_baseline"] = cpu
     print(json.dumps(out), flush=True)
@@ -431,6 +454,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=10.0,
+                    help="length of the serving replay at N=1 (0 = skip)")
+    ap.add_argument("--serve-rate", type=float, default=200_000.0, help="serving arrivals per second")
+    ap.add_argument("--serve-streams", type=int, default=4, help="serving batches in flight")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

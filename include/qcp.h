@@ -196,6 +196,45 @@ qcp_status qcp_index_export(const qcp_index* index, uint64_t* keys, int32_t* ids
 qcp_status qcp_query_counts_noalloc(qcp_index* index, const float* d_boxes, uint32_t q,
                                     uint64_t* d_counts, void* stream);
 
+/* Serving: replays an open-loop arrival trace through continuous batching
+ * over the resident index.  Request i (box i, q rows of 2*dims floats in
+ * host memory) arrives arrival_s[i] seconds after the call starts
+ * (non-decreasing).  `streams` worker threads, each with its own CUDA stream,
+ * take every request that has arrived (up to max_batch), count their hits
+ * and admit the longest prefix whose result bytes (4 per id + 8 per query)
+ * fit output_cap_bytes next to the results other workers hold -- a request
+ * larger than the cap runs alone -- then run it as one sorted batch; batches
+ * of different workers overlap on the device.  deliver (optional) receives
+ * every request's ascending ids, from the worker threads, once each.
+ * latency_ms (optional, q entries) gets arrival -> results-on-host time per
+ * request.  No counterpart in the reference (its Evaluator replays fixed
+ * query files through Tree::Search, src/evaluator/evaluator.cpp:171-280). */
+typedef void (*qcp_deliver_fn)(void* user, uint32_t request, const int32_t* ids, uint64_t n);
+
+typedef struct qcp_serve_opts {
+  uint32_t streams;          /* batches in flight; 0 = 4 */
+  uint32_t max_batch;        /* queries per batch at most; 0 = 16384 */
+  uint64_t output_cap_bytes; /* result bytes held at once; 0 = 2 GiB */
+  qcp_deliver_fn deliver;    /* NULL: results are dropped after the copy */
+  void* user;                /* passed to deliver */
+} qcp_serve_opts;
+
+typedef struct qcp_serve_stats {
+  uint64_t requests;
+  uint64_t hits;
+  uint64_t batches;
+  double mean_batch;         /* requests per batch */
+  double seconds;            /* first arrival -> last completion */
+  double qps;                /* requests / seconds */
+  double p50_ms, p99_ms, max_ms, mean_ms;  /* with latency_ms only */
+  uint32_t max_inflight;     /* most batches on the device at once */
+  uint32_t reserved_;
+  uint64_t max_output_bytes; /* most result bytes held at once */
+} qcp_serve_stats;
+
+qcp_status qcp_serve_replay(qcp_index* index, const float* boxes, const double* arrival_s, uint32_t q,
+                            const qcp_serve_opts* opts, float* latency_ms, qcp_serve_stats* stats);
+
 /* Message of the last error on the calling host thread ("" if none). */
 const char* qcp_last_error(void);
 

@@ -74,6 +74,24 @@ class QueryStats(ctypes.Structure):
                 ("ms_sort_windows", ctypes.c_float), ("sort_window_ids", ctypes.c_uint64)]
 
 
+DELIVER_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int32),
+                              ctypes.c_uint64)
+
+
+class ServeOpts(ctypes.Structure):
+    _fields_ = [("streams", ctypes.c_uint32), ("max_batch", ctypes.c_uint32),
+                ("output_cap_bytes", ctypes.c_uint64), ("deliver", DELIVER_FN),
+                ("user", ctypes.c_void_p)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("requests", ctypes.c_uint64), ("hits", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("mean_batch", ctypes.c_double), ("seconds", ctypes.c_double), ("qps", ctypes.c_double),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("max_inflight", ctypes.c_uint32),
+                ("reserved_", ctypes.c_uint32), ("max_output_bytes", ctypes.c_uint64)]
+
+
 class Result(ctypes.Structure):
     _fields_ = [("num_queries", ctypes.c_uint32), ("mem", ctypes.c_uint32),
                 ("total_hits", ctypes.c_uint64), ("offsets", ctypes.c_void_p),
@@ -108,6 +126,8 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
         "qcp_launch_count": ([ctypes.c_int], U64),
         "qcp_version": ([], ctypes.c_char_p),
         "qcp_query_stats_last": ([ctypes.POINTER(QueryStats)], ctypes.c_int),
+        "qcp_serve_replay": ([P, P, P, U32, ctypes.POINTER(ServeOpts), P, ctypes.POINTER(ServeStats)],
+                             ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -310,6 +330,39 @@ class Index:
         opts = self._opts(algo, bmem, MEM_HOST, True, stream)
         _check(lib.qcp_query_counts(self._h, ptr, nq, ctypes.byref(opts), _ptr(out)))
         return out
+
+
+    def serve(self, boxes, arrival_s, streams: int = 4, max_batch: int = 16384,
+              output_cap_bytes: int = 2 << 30, collect: bool = False):
+        """Replay an open-loop arrival trace through the library's continuous
+        batching loop (qcp_serve_replay).  boxes: (q, 2*dims) float32 host
+        array; arrival_s: non-decreasing arrival times in seconds.  Returns
+        (stats dict, per-request latency in ms, per-request id arrays or
+        None when collect is False)."""
+        lib = load_library()
+        b = np.ascontiguousarray(boxes, dtype=np.float32).reshape(-1, 2 * self.dims)
+        t = np.ascontiguousarray(arrival_s, dtype=np.float64)
+        if t.shape[0] != b.shape[0]:
+            raise ValueError("one arrival time per box")
+        lat = np.zeros(b.shape[0], np.float32)
+        got = [None] * b.shape[0] if collect else None
+        opts = ServeOpts()
+        opts.streams, opts.max_batch, opts.output_cap_bytes = streams, max_batch, output_cap_bytes
+        if collect:
+            import threading
+            lock = threading.Lock()
+
+            def _deliver(_user, req, ids, n):
+                a = np.ctypeslib.as_array(ids, shape=(int(n),)).copy() if n else np.zeros(0, np.int32)
+                with lock:
+                    got[req] = a
+            cb = DELIVER_FN(_deliver)
+            opts.deliver = cb
+        st = ServeStats()
+        _check(lib.qcp_serve_replay(self._h, _ptr(b), _ptr(t), b.shape[0], ctypes.byref(opts), _ptr(lat),
+                                    ctypes.byref(st)))
+        stats = {k: getattr(st, k) for k, _ in ServeStats._fields_ if k != "reserved_"}
+        return stats, lat, got
 
 
 def last_stats() -> dict:

@@ -18,6 +18,8 @@
 #include <cfloat>
 #include <cmath>
 
+#include <mutex>
+
 #include "qcp_internal.cuh"
 
 namespace qcp {
@@ -395,12 +397,42 @@ int num_sms() {
   return sms;
 }
 
+// Temporaries freed before the work that uses them has run are taken from
+// the device's stream-ordered pool (cudaMallocAsync / cudaFreeAsync): a
+// buffer freed on one stream is handed to another stream only after the
+// freeing stream has reached the free, so calls that run concurrently on
+// different streams never share one.  The pool keeps what it caches.
+qcp_status temp_alloc(size_t bytes, cudaStream_t s, void** out) {
+  int dev = 0;
+  QCP_CUDA(cudaGetDevice(&dev));
+  static std::mutex mu;
+  static bool kept[64] = {};
+  if (dev >= 0 && dev < 64) {
+    std::lock_guard<std::mutex> g(mu);
+    if (!kept[dev]) {
+      cudaMemPool_t mp;
+      if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+      kept[dev] = true;
+    }
+  }
+  QCP_CUDA(cudaMallocAsync(out, bytes ? bytes : 1, s));
+  return QCP_OK;
+}
+
+void temp_free(void* p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
 template <class T>
 qcp_status exclusive_scan(const T* in, T* out, uint64_t n, T* grand_total, DevPool& pool,
                           cudaStream_t s) {
+  (void)pool;
   const uint32_t nblk = (uint32_t)((n + SC_CHUNK - 1) / SC_CHUNK);
   void* sums = nullptr;
-  QCP_TRY(pool.get(sizeof(T) * (nblk ? nblk : 1), &sums));
+  QCP_TRY(temp_alloc(sizeof(T) * (nblk ? nblk : 1), s, &sums));
   if (n) {
     k_scan_sums<T><<<nblk, SC_THREADS, 0, s>>>(in, n, (T*)sums);
     k_scan_partials<T><<<1, 1024, 0, s>>>((T*)sums, nblk, grand_total);
@@ -408,7 +440,7 @@ qcp_status exclusive_scan(const T* in, T* out, uint64_t n, T* grand_total, DevPo
     note_launch(3);
   }
   qcp_status st = check_launch("exclusive_scan");
-  pool.put(sizeof(T) * (nblk ? nblk : 1), sums);
+  temp_free(sums, s);
   return st;
 }
 
@@ -435,10 +467,10 @@ qcp_status radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, 
   const uint64_t hn = 256ull * ntiles;
   void* hist = nullptr;
   void* offs = nullptr;
-  QCP_TRY(pool.get(sizeof(uint32_t) * hn, &hist));
-  qcp_status st = pool.get(sizeof(uint32_t) * hn, &offs);
+  QCP_TRY(temp_alloc(sizeof(uint32_t) * hn, s, &hist));
+  qcp_status st = temp_alloc(sizeof(uint32_t) * hn, s, &offs);
   if (st != QCP_OK) {
-    pool.put(sizeof(uint32_t) * hn, hist);
+    temp_free(hist, s);
     return st;
   }
   uint64_t* kin = keys;
@@ -460,8 +492,8 @@ qcp_status radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, 
     std::swap(vin, vout);
     *result_in_tmp = !*result_in_tmp;
   }
-  pool.put(sizeof(uint32_t) * hn, hist);
-  pool.put(sizeof(uint32_t) * hn, offs);
+  temp_free(hist, s);
+  temp_free(offs, s);
   return st;
 }
 
