@@ -105,6 +105,12 @@ typedef struct qcp_query_opts {
   uint32_t unsorted;   /* 1 = skip the per-query id sort (hit SET still exact) */
   void* stream;        /* cudaStream_t; NULL = legacy default stream */
   uint32_t flags;      /* QCP_QUERY_* bits */
+  /* Tuning knobs (0 = default; qcp_autotune picks them): CUDA blocks per SM
+   * of the batched traversal kernels (default 8, at most 32), and log2 of
+   * the id window of the per-query sort (default and largest 18, smallest
+   * 12; raised where the id range would need more than 8192 windows). */
+  uint32_t blocks_per_sm;
+  uint32_t win_bits;
   uint32_t reserved_;
 } qcp_query_opts;
 
@@ -195,6 +201,34 @@ qcp_status qcp_index_export(const qcp_index* index, uint64_t* keys, int32_t* ids
  * (split the batch).  No counterpart in the reference. */
 qcp_status qcp_query_counts_noalloc(qcp_index* index, const float* d_boxes, uint32_t q,
                                     uint64_t* d_counts, void* stream);
+
+/* Autotuner: picks the build fan-out and the query knobs (blocks_per_sm,
+ * win_bits) for a data set and a sample of its queries by timing trials on
+ * the current device: every fan-out in {64, 128, 256} is built and queried
+ * with the default knobs, then blocks_per_sm in {4, 8, 16} and win_bits in
+ * {16, 17, 18} are tried one after the other at the best fan-out (coordinate
+ * descent); each trial is the median of `repeats` timed batches of the
+ * sample (sorted output) after one untimed batch.  objs and boxes are host
+ * memory as for qcp_index_build / qcp_query_batch; `base` supplies the key
+ * mode, key bits and stream (its fanout is ignored).  The reference fixes
+ * its fan-out at compile time (NODE_SIZE, src/common/config.h) and has no
+ * tuner. */
+#define QCP_TUNE_MAX_TRIALS 16
+typedef struct qcp_tune_result {
+  uint32_t fanout;            /* best build fan-out */
+  uint32_t blocks_per_sm;     /* best qcp_query_opts.blocks_per_sm */
+  uint32_t win_bits;          /* best qcp_query_opts.win_bits */
+  uint32_t trials;            /* entries used in the arrays below */
+  float best_ms;              /* batch time of the best trial */
+  float build_ms;             /* build time at the best fan-out */
+  uint32_t trial_fanout[QCP_TUNE_MAX_TRIALS];
+  uint32_t trial_blocks_per_sm[QCP_TUNE_MAX_TRIALS];
+  uint32_t trial_win_bits[QCP_TUNE_MAX_TRIALS];
+  float trial_ms[QCP_TUNE_MAX_TRIALS];
+} qcp_tune_result;
+
+qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims, uint32_t is_rect, const float* boxes,
+                        uint32_t q, const qcp_build_opts* base, uint32_t repeats, qcp_tune_result* out);
 
 /* Serving: replays an open-loop arrival trace through continuous batching
  * over the resident index.  Request i (box i, q rows of 2*dims floats in

@@ -55,6 +55,7 @@ class QueryOpts(ctypes.Structure):
     _fields_ = [("algo", ctypes.c_uint32), ("boxes_mem", ctypes.c_uint32),
                 ("result_mem", ctypes.c_uint32), ("unsorted", ctypes.c_uint32),
                 ("stream", ctypes.c_void_p), ("flags", ctypes.c_uint32),
+                ("blocks_per_sm", ctypes.c_uint32), ("win_bits", ctypes.c_uint32),
                 ("reserved_", ctypes.c_uint32)]
 
 
@@ -90,6 +91,19 @@ class ServeStats(ctypes.Structure):
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
                 ("mean_ms", ctypes.c_double), ("max_inflight", ctypes.c_uint32),
                 ("reserved_", ctypes.c_uint32), ("max_output_bytes", ctypes.c_uint64)]
+
+
+TUNE_MAX_TRIALS = 16
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("fanout", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32),
+                ("win_bits", ctypes.c_uint32), ("trials", ctypes.c_uint32),
+                ("best_ms", ctypes.c_float), ("build_ms", ctypes.c_float),
+                ("trial_fanout", ctypes.c_uint32 * TUNE_MAX_TRIALS),
+                ("trial_blocks_per_sm", ctypes.c_uint32 * TUNE_MAX_TRIALS),
+                ("trial_win_bits", ctypes.c_uint32 * TUNE_MAX_TRIALS),
+                ("trial_ms", ctypes.c_float * TUNE_MAX_TRIALS)]
 
 
 class Result(ctypes.Structure):
@@ -128,6 +142,8 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
         "qcp_query_stats_last": ([ctypes.POINTER(QueryStats)], ctypes.c_int),
         "qcp_serve_replay": ([P, P, P, U32, ctypes.POINTER(ServeOpts), P, ctypes.POINTER(ServeStats)],
                              ctypes.c_int),
+        "qcp_autotune": ([P, U64, U32, U32, P, U32, ctypes.POINTER(BuildOpts), U32, ctypes.POINTER(TuneResult)],
+                         ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -273,14 +289,14 @@ class Index:
         return keys, ids, mbr
 
     # -- queries --------------------------------------------------------------
-    def _opts(self, algo, boxes_mem, result_mem, sort, stream, timing=False):
+    def _opts(self, algo, boxes_mem, result_mem, sort, stream, timing=False, blocks_per_sm=0, win_bits=0):
         a = {"batched": ALGO_BATCHED, "plain": ALGO_PLAIN}.get(algo, algo)
         return QueryOpts(a, boxes_mem, result_mem, 0 if sort else 1, ctypes.c_void_p(stream or None),
-                         QUERY_TIMING if timing else 0, 0)
+                         QUERY_TIMING if timing else 0, blocks_per_sm, win_bits, 0)
 
     def search(self, boxes, algo="batched", sort: bool = True, result_mem: int = MEM_HOST,
                q: int | None = None, stream: int = 0, timing: bool = False,
-               copy: bool = True) -> SearchResult:
+               copy: bool = True, blocks_per_sm: int = 0, win_bits: int = 0) -> SearchResult:
         """Run a batch of box queries.  Host numpy boxes (q x 2D) or a CUDA
         tensor/pointer (then pass q).  Host results are copied into numpy
         arrays (copy=False: numpy views of the library's pinned result arena,
@@ -294,7 +310,7 @@ class Index:
             if q is None:
                 raise ValueError("device boxes need q")
             b, nq, ptr, bmem = boxes, q, ctypes.c_void_p(_device_ptr(boxes)), MEM_DEVICE
-        opts = self._opts(algo, bmem, result_mem, sort, stream, timing)
+        opts = self._opts(algo, bmem, result_mem, sort, stream, timing, blocks_per_sm, win_bits)
         r = Result()
         _check(lib.qcp_query_batch(self._h, ptr, nq, ctypes.byref(opts), ctypes.byref(r)))
         if result_mem == MEM_HOST and not copy:
@@ -363,6 +379,26 @@ class Index:
                                     ctypes.byref(st)))
         stats = {k: getattr(st, k) for k, _ in ServeStats._fields_ if k != "reserved_"}
         return stats, lat, got
+
+
+def autotune(objs, boxes, is_rect: bool = False, dims: int | None = None, key_mode: int = 0,
+             repeats: int = 3) -> dict:
+    """Pick the fan-out and the query knobs (blocks_per_sm, win_bits) for a
+    data set and a sample of its queries by timed trials (qcp_autotune).
+    Returns the choice, its batch time and every trial."""
+    o = np.ascontiguousarray(objs, dtype=np.float32)
+    d = dims or (o.shape[1] // 2 if is_rect else o.shape[1])
+    b = np.ascontiguousarray(boxes, dtype=np.float32).reshape(-1, 2 * d)
+    bo = BuildOpts()
+    bo.key_mode = key_mode
+    r = TuneResult()
+    _check(load_library().qcp_autotune(_ptr(o), o.shape[0], d, int(is_rect), _ptr(b), b.shape[0],
+                                       ctypes.byref(bo), repeats, ctypes.byref(r)))
+    n = r.trials
+    return {"fanout": r.fanout, "blocks_per_sm": r.blocks_per_sm, "win_bits": r.win_bits,
+            "best_ms": r.best_ms, "build_ms": r.build_ms,
+            "trials": [{"fanout": r.trial_fanout[i], "blocks_per_sm": r.trial_blocks_per_sm[i],
+                        "win_bits": r.trial_win_bits[i], "ms": r.trial_ms[i]} for i in range(n)]}
 
 
 def last_stats() -> dict:

@@ -106,6 +106,8 @@ struct Workspace {
   cudaEvent_t ev[kEvCountSlots] = {};
   bool timing = false;
   bool sort_part_marked = false;
+  uint32_t blocks_per_sm = 8;    // traversal grid = SMs x this, this call
+  uint32_t win_bits = 18;        // sort window, this call
   uint32_t sort_small_jobs = 0, sort_msd_jobs = 0;
 };
 

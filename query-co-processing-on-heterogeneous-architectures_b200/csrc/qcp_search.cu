@@ -369,7 +369,7 @@ qcp_status init_items(Workspace* ws, uint32_t q, cudaStream_t s) {
 
 qcp_status expand_level(qcp_index* ix, Workspace* ws, uint32_t l, int cur, cudaStream_t s) {
   const TreeView t = view_of(ix);
-  const uint32_t grid = (uint32_t)num_sms() * 8;  // 8 x 256 threads resident per SM
+  const uint32_t grid = (uint32_t)num_sms() * ws->blocks_per_sm;
   const int nxt = cur ^ 1;
   uint32_t* ctr = ws->ctr;
   QCP_DISPATCH_D(ix->dims, launch_expand<DD>(grid, s, ws->boxes, ws->items[cur], ctr + kCtrFrontier0 + cur,
@@ -382,7 +382,7 @@ qcp_status expand_level(qcp_index* ix, Workspace* ws, uint32_t l, int cur, cudaS
 
 qcp_status write_items(qcp_index* ix, Workspace* ws, int cur, cudaStream_t s) {
   const TreeView t = view_of(ix);
-  const uint32_t grid = (uint32_t)num_sms() * 8;
+  const uint32_t grid = (uint32_t)num_sms() * ws->blocks_per_sm;
   uint32_t* ctr = ws->ctr;
   QCP_DISPATCH_D(ix->dims, launch_leafscan<DD, kWrite>(ix->is_rect != 0, grid, s, t, ws->boxes, ws->items[cur],
                                                        ctr + kCtrFrontier0 + cur, ctr + kCtrWork,
@@ -398,7 +398,7 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
   const uint32_t D = ix->dims;
   const bool rect = ix->is_rect != 0;
   const uint32_t sms = (uint32_t)num_sms();
-  const uint32_t grid = sms * 8;  // 8 x 256 threads resident per SM
+  const uint32_t grid = sms * ws->blocks_per_sm;  // 256-thread blocks
   uint32_t* ctr = ws->ctr;
   // start level: items at level `start` are (query, node) pairs
   const uint32_t start = (ix->levels >= 2) ? ix->levels - 1 : 1;

@@ -532,7 +532,12 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   Job* big = const_cast<Job*>(bigc);
   uint32_t* ctr = ws->ctr;
   const uint32_t idbits = id_bits(ix->n);
-  const uint32_t wbits = idbits < kWinBits ? idbits : kWinBits;
+  // window bits of this call: at most kWinBits (the bitmap), at least what
+  // keeps the window count <= 8192 (the scatter's shared counters)
+  uint32_t wb = ws->win_bits ? ws->win_bits : kWinBits;
+  if (wb > kWinBits) wb = kWinBits;
+  if (idbits > 13 && wb < idbits - 13) wb = idbits - 13;
+  const uint32_t wbits = idbits < wb ? idbits : wb;
   const uint32_t G = 1u << (idbits - wbits);
   const uint32_t sms = (uint32_t)num_sms();
   const size_t rank_bytes = sizeof(RankSmem);
