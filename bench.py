@@ -169,6 +169,18 @@ def run_ours(args, rank, world, local):
     sp = stream.cuda_stream
     torch.cuda.synchronize()
 
+    # ---- autotune on a separate query sample of the same distribution -------
+    knobs = {"fanout": args.fanout, "blocks_per_sm": 0, "win_bits": 0}
+    tune = None
+    if args.algo == "batched" and not args.no_tune:
+        if args.workload == "uniform1m":
+            sample = W.fixed_cubes(2000, 3, 0.0464, seed=W.QUERY_SEED + 77)
+        else:
+            sample = W.data_centred_cubes(w.objs, 2000, 1e-6, 1e-2, seed=W.QUERY_SEED + 77)
+        tune = qcp.autotune(w.objs, sample, repeats=2)
+        knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits")}
+    args.fanout = knobs["fanout"]
+
     t0 = time.perf_counter()
     ix = qcp.Index.build(d_objs, dims=w.dims, n=w.n, fanout=args.fanout, stream=sp)
     build_ms = (time.perf_counter() - t0) * 1e3
@@ -187,7 +199,8 @@ def run_ours(args, rank, world, local):
         return float(t.item())
 
     def step_device(algo, timing):
-        r = ix.search(d_boxes, q=Q, algo=algo, result_mem=qcp.MEM_DEVICE, stream=sp, timing=timing)
+        r = ix.search(d_boxes, q=Q, algo=algo, result_mem=qcp.MEM_DEVICE, stream=sp, timing=timing,
+                      blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"])
         hits = r.total_hits
         r.release()
         return hits
@@ -263,7 +276,8 @@ def run_ours(args, rank, world, local):
     d2h = 0
 
     def step_host():
-        r = ix.search(h_np, algo=args.algo, result_mem=qcp.MEM_HOST, stream=sp, copy=False)
+        r = ix.search(h_np, algo=args.algo, result_mem=qcp.MEM_HOST, stream=sp, copy=False,
+                      blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"])
         nb = (Q + 1) * 8 + r.total_hits * 4
         r.release()
         return nb
@@ -331,7 +345,12 @@ def run_ours(args, rank, world, local):
         "config": {
             "workload": f"{w.name}: {w.n} 3-D points, {Q} queries per GPU per step"
                         if args.workload != "uniform1m" else f"{w.name}",
-            "fanout": args.fanout, "algo": args.algo, "queries_per_step_per_gpu": Q,
+            "fanout": args.fanout, "blocks_per_sm": knobs["blocks_per_sm"] or 8,
+            "win_bits": knobs["win_bits"] or 18,
+            "tuned": None if tune is None else {"sample_queries": 2000, "best_ms": round(tune["best_ms"], 3),
+                                                "trials": [[t["fanout"], t["blocks_per_sm"], t["win_bits"],
+                                                            round(t["ms"], 3)] for t in tune["trials"]]},
+            "algo": args.algo, "queries_per_step_per_gpu": Q,
             "n_objects": w.n, "key": f"hilbert {info['key_bits']} bits/dim",
             "levels": info["levels"], "index_bytes": info["device_bytes"],
             "l2": "inputs larger than L2 (index %.0f MB, %.0f MB of ids written per step)"
@@ -454,6 +473,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (use --fanout and defaults)")
     ap.add_argument("--serve-seconds", type=float, default=10.0,
                     help="length of the serving replay at N=1 (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=200_000.0, help="serving arrivals per second")
