@@ -115,7 +115,7 @@ def dist_setup(n_gpus):
     return rank, world, local
 
 
-def algorithmic_bytes(st: dict, dims: int, fanout: int) -> dict:
+def algorithmic_bytes(st: dict, dims: int, fanout: int, is_rect: bool = False) -> dict:
     """Bytes each kernel must move at minimum for the work it did, per launch
     (one launch of each per step):
     k_leafscan<count>  leaf-MBR reads of every (query, leaf-parent) item +
@@ -125,7 +125,7 @@ def algorithmic_bytes(st: dict, dims: int, fanout: int) -> dict:
     k_win_sort         4 B read + 4 B write per id of the larger slices
     """
     mbr = st["leaf_items"] * fanout * 2 * dims * 4
-    coords = st["leaves_partial"] * fanout * dims * 4
+    coords = st["leaves_partial"] * fanout * (2 if is_rect else 1) * dims * 4
     hits = st["hits"]
     win = st["sort_window_ids"]
     return {"count": mbr + coords, "write": mbr + coords + 8 * hits,
@@ -136,6 +136,34 @@ def algorithmic_bytes(st: dict, dims: int, fanout: int) -> dict:
 # 16M-point Gaussian workload at 2,000 queries (profiles/k_win_sort_gauss16m_q2000.md),
 # applied to the ids of the timed launch: traffic grows with the ids processed.
 K_WIN_SORT_DRAM_BYTES_PER_ID = (851630848 + 797769216) / 211501325  # 7.80 B per id
+
+
+def load_workload(W, name, queries, world):
+    """(workload, query boxes of all ranks) for a workload name."""
+    if name == "uniform1m":
+        w = W.config1()
+        return w, W.fixed_cubes((queries or 1000) * world, 3, 0.0464)
+    if name == "uniform2d64m":
+        w = W.config3()
+        q = (queries or 100_000) * world
+        return w, W.fixed_cubes(q, 2, float(np.sqrt(1e-5)))
+    if name == "rect8d32m":
+        w = W.config4()
+        return w, W.rect8d_boxes((queries or 50_000) * world)
+    w = W.config2(q=(queries or 10_000) * world)
+    return w, w.boxes
+
+
+def tune_sample(W, name, w, n=2000):
+    """A query sample of the workload's distribution, with its own seed."""
+    seed = W.QUERY_SEED + 77
+    if name == "uniform1m":
+        return W.fixed_cubes(n, 3, 0.0464, seed=seed)
+    if name == "uniform2d64m":
+        return W.fixed_cubes(n, 2, float(np.sqrt(1e-5)), seed=seed)
+    if name == "rect8d32m":
+        return W.rect8d_boxes(n, seed=seed)
+    return W.data_centred_cubes(w.objs, n, 1e-6, 1e-2, seed=seed)
 
 
 def run_ours(args, rank, world, local):
@@ -151,13 +179,7 @@ def run_ours(args, rank, world, local):
     dev = torch.device("cuda", local)
 
     # ---- workload (identical on every rank) --------------------------------
-    q_per_rank = args.queries
-    if args.workload == "uniform1m":
-        w = W.config1()
-        boxes_all = W.fixed_cubes(q_per_rank * world, 3, 0.0464)
-    else:
-        w = W.config2(q=q_per_rank * world)
-        boxes_all = w.boxes
+    w, boxes_all = load_workload(W, args.workload, args.queries, world)
     import qcp_b200.sharding as S
     a, b = S.query_shard(len(boxes_all), rank, world)
     boxes = np.ascontiguousarray(boxes_all[a:b])
@@ -173,16 +195,13 @@ def run_ours(args, rank, world, local):
     knobs = {"fanout": args.fanout, "blocks_per_sm": 0, "win_bits": 0}
     tune = None
     if args.algo == "batched" and not args.no_tune:
-        if args.workload == "uniform1m":
-            sample = W.fixed_cubes(2000, 3, 0.0464, seed=W.QUERY_SEED + 77)
-        else:
-            sample = W.data_centred_cubes(w.objs, 2000, 1e-6, 1e-2, seed=W.QUERY_SEED + 77)
-        tune = qcp.autotune(w.objs, sample, repeats=2)
+        sample = tune_sample(W, args.workload, w)
+        tune = qcp.autotune(w.objs, sample, is_rect=w.is_rect, dims=w.dims, repeats=2)
         knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits")}
     args.fanout = knobs["fanout"]
 
     t0 = time.perf_counter()
-    ix = qcp.Index.build(d_objs, dims=w.dims, n=w.n, fanout=args.fanout, stream=sp)
+    ix = qcp.Index.build(d_objs, dims=w.dims, n=w.n, is_rect=w.is_rect, fanout=args.fanout, stream=sp)
     build_ms = (time.perf_counter() - t0) * 1e3
     info = ix.info()
     del d_objs
@@ -244,7 +263,7 @@ def run_ours(args, rank, world, local):
     hbm, peak_kind = peaks()
     kernel_names = {"count": "k_leafscan<count>", "write": "k_leafscan<write>",
                     "sort_small": "k_sort_small", "sort_windows": "k_win_sort"}
-    ab = algorithmic_bytes(stats, w.dims, args.fanout)
+    ab = algorithmic_bytes(stats, w.dims, args.fanout, w.is_rect)
     dominant = max(kernel_names, key=lambda k: phase[k])
     per_launch_ms = phase[dominant] / args.steps
     achieved = ab[dominant] / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
@@ -298,7 +317,7 @@ def run_ours(args, rank, world, local):
 
     # ---- serving: open-loop Poisson arrivals through continuous batching ----
     serving = None
-    if args.serve_seconds > 0 and world == 1:
+    if args.serve_seconds > 0 and world == 1 and args.workload == "gauss16m":
         t_arr, s_boxes, s_cls = W.serving_stream(w.objs, rate=args.serve_rate, duration_s=args.serve_seconds)
         # warm-up: a burst at t = 0 sizes every stream's workspace for full
         # batches, then a short open-loop run
@@ -320,7 +339,11 @@ def run_ours(args, rank, world, local):
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w.objs, boxes, args.cpu_seconds)
+        if w.is_rect:
+            cpu = {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
+                   "sample": "unavailable: the reference's data path loads points only"}
+        else:
+            cpu = cpu_baseline(w.objs, boxes, args.cpu_seconds, w.dims)
 
     ix.close()
     if world > 1:
@@ -343,8 +366,8 @@ def run_ours(args, rank, world, local):
         "dtype": "f32",
         "data": "synthetic (seeded numpy PCG64; no public dataset)",
         "config": {
-            "workload": f"{w.name}: {w.n} 3-D points, {Q} queries per GPU per step"
-                        if args.workload != "uniform1m" else f"{w.name}",
+            "workload": f"{w.name}: {w.n} {w.dims}-D {'rectangles' if w.is_rect else 'points'}, "
+                        f"{Q} queries per GPU per step",
             "fanout": args.fanout, "blocks_per_sm": knobs["blocks_per_sm"] or 8,
             "win_bits": knobs["win_bits"] or 18,
             "tuned": None if tune is None else {"sample_queries": 2000, "best_ms": round(tune["best_ms"], 3),
@@ -385,18 +408,18 @@ def run_ours(args, rank, world, local):
     print(json.dumps(out), flush=True)
 
 
-def _reference_lib():
+def _reference_lib(dims: int = 3):
     sys.path.insert(0, str(ROOT / "oracle"))
     from oracle import Reference  # test infrastructure: the timed reference
-    if not Reference.available(3):
+    if not Reference.available(dims):
         return None
-    return Reference(3)
+    return Reference(dims)
 
 
-def cpu_baseline(objs, boxes, seconds):
+def cpu_baseline(objs, boxes, seconds, dims=3):
     """The reference's CPU BVH traversal on this host's cores over a bounded
     sample of the batch (as many queries as fit in about `seconds`)."""
-    ref = _reference_lib()
+    ref = _reference_lib(dims)
     if ref is None:
         return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
                 "sample": "unavailable: oracle/_ref not built"}
@@ -419,11 +442,12 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     import qcp_b200.workloads as W  # noqa: F401  (package import below)
-    ref = _reference_lib()
-    if args.workload == "uniform1m":
-        w = W.config1()
-    else:
-        w = W.config2(q=args.queries)
+    w, _ = load_workload(W, args.workload, args.queries, 1)
+    if w.is_rect:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "the reference's data path loads points only; this workload is rectangles"}))
+        return
+    ref = _reference_lib(w.dims)
     if ref is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libqcpref_d3.so not built"}))
         return
@@ -449,7 +473,7 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / len(times) * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded numpy PCG64; no public dataset)",
-        "config": {"workload": f"{w.name}: {w.n} 3-D points; each step the first {n} queries of the batch",
+        "config": {"workload": f"{w.name}: {w.n} {w.dims}-D points; each step the first {n} queries of the batch",
                    "fanout": "reference BVH, <=128 per node"},
         "cpu_baseline": {"value": round(value, 1), "unit": "queries/s", "cores": threads,
                          "kind": "reference",
@@ -466,8 +490,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--algo", default="batched", choices=["batched", "plain"])
-    ap.add_argument("--workload", default="gauss16m", choices=["gauss16m", "uniform1m"])
-    ap.add_argument("--queries", type=int, default=10_000)
+    ap.add_argument("--workload", default="gauss16m",
+                    choices=["gauss16m", "uniform1m", "uniform2d64m", "rect8d32m"],
+                    help="gauss16m: 16M clustered 3-D points; uniform1m: 1M uniform 3-D points; "
+                         "uniform2d64m: 64M uniform 2-D points (64-bit keys); rect8d32m: 32M 8-D rectangles")
+    ap.add_argument("--queries", type=int, default=None,
+                    help="queries per GPU per step (default: the workload's own count; 10,000 for gauss16m)")
     ap.add_argument("--fanout", type=int, default=128)
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=3)

@@ -127,10 +127,15 @@ def config4(scale: float = 1.0) -> Workload:
     side = rng.exponential(0.002, size=(n, 8)).astype(np.float32)
     objs = np.ascontiguousarray(np.concatenate([lo, (lo + side).astype(np.float32)], axis=1))
     q = max(1, int(50_000 * min(1.0, scale * 10)))
-    qr = np.random.Generator(np.random.PCG64(QUERY_SEED))
+    return Workload("rect8d_32M_q50k", 8, True, objs, rect8d_boxes(q), fanout=128)
+
+
+def rect8d_boxes(q: int, seed: int = QUERY_SEED) -> np.ndarray:
+    """q 8-D boxes: centre U[0,1)^8, side per dimension U[0.05, 0.2]."""
+    qr = np.random.Generator(np.random.PCG64(seed))
     centres = qr.random((q, 8), dtype=np.float32)
     sides = qr.uniform(0.05, 0.2, size=(q, 8)).astype(np.float32)
-    return Workload("rect8d_32M_q50k", 8, True, objs, _cubes(centres, sides), fanout=128)
+    return _cubes(centres, sides)
 
 
 def serving_stream(objs: np.ndarray, rate: float = 200_000.0, duration_s: float = 10.0,
