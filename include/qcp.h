@@ -230,6 +230,36 @@ typedef struct qcp_tune_result {
 qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims, uint32_t is_rect, const float* boxes,
                         uint32_t q, const qcp_build_opts* base, uint32_t repeats, qcp_tune_result* out);
 
+/* Query plans: the batched pipeline (sorted ids unless opts->unsorted) for at
+ * most max_queries boxes and max_hits ids per batch, captured once into a
+ * CUDA graph and replayed per batch.  qcp_query_batch sizes its buffers and
+ * launches from host readbacks between its phases; a plan fixes them at
+ * creation (device memory for max_queries boxes, the frontier, max_hits ids
+ * twice, the sort's tables) so every phase runs from device-resident counts,
+ * and one graph launch replaces its ~20 kernel launches and 3 host round
+ * trips.  opts: blocks_per_sm, win_bits and unsorted are used (algo must be
+ * batched; NULL = defaults).  qcp_plan_create runs the pipeline once on an
+ * empty batch before capturing it.
+ *
+ * qcp_plan_run: boxes (q <= max_queries rows, host or device memory per
+ * boxes_mem) are copied in and the batch is padded with empty boxes; on
+ * return *total_hits is set and *d_offsets (q + 1 entries) / *d_ids point to
+ * the plan's device result, valid until the next run or qcp_plan_free.  A
+ * batch whose hits exceed max_hits, or whose traversal frontier exceeds the
+ * plan's item capacity (64 per query + 1 per 1024 hits + 65536), returns
+ * QCP_ERR_OUTPUT_OVERFLOW (run it through qcp_query_batch or a larger plan).
+ * A plan runs one batch at a time; plans of one index may run concurrently
+ * on different streams.  The reference launches one kernel per 128 queries
+ * with host synchronisation in between (MPHR::Search,
+ * src/tree/mphr.cpp:231-258). */
+typedef struct qcp_plan qcp_plan;
+
+qcp_status qcp_plan_create(qcp_index* index, uint32_t max_queries, uint64_t max_hits,
+                           const qcp_query_opts* opts, qcp_plan** out);
+qcp_status qcp_plan_run(qcp_plan* plan, const float* boxes, uint32_t q, uint32_t boxes_mem, void* stream,
+                        uint64_t* total_hits, const uint64_t** d_offsets, const int32_t** d_ids);
+qcp_status qcp_plan_free(qcp_plan* plan);
+
 /* Serving: replays an open-loop arrival trace through continuous batching
  * over the resident index.  Request i (box i, q rows of 2*dims floats in
  * host memory) arrives arrival_s[i] seconds after the call starts

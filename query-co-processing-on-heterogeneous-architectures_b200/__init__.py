@@ -144,6 +144,10 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
                              ctypes.c_int),
         "qcp_autotune": ([P, U64, U32, U32, P, U32, ctypes.POINTER(BuildOpts), U32, ctypes.POINTER(TuneResult)],
                          ctypes.c_int),
+        "qcp_plan_create": ([P, U32, U64, ctypes.POINTER(QueryOpts), ctypes.POINTER(P)], ctypes.c_int),
+        "qcp_plan_run": ([P, P, U32, U32, P, ctypes.POINTER(U64), ctypes.POINTER(P), ctypes.POINTER(P)],
+                         ctypes.c_int),
+        "qcp_plan_free": ([P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -379,6 +383,60 @@ class Index:
                                     ctypes.byref(st)))
         stats = {k: getattr(st, k) for k, _ in ServeStats._fields_ if k != "reserved_"}
         return stats, lat, got
+
+
+class _DeviceArray:
+    """A device buffer described by __cuda_array_interface__ (read-only view)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3}
+
+
+class Plan:
+    """A captured query pipeline for batches of at most max_queries boxes and
+    max_hits ids (qcp_plan_create).  run() returns host copies of the
+    offsets and ids; run_device() the plan's device pointers."""
+
+    def __init__(self, index: "Index", max_queries: int, max_hits: int, sort: bool = True,
+                 blocks_per_sm: int = 0, win_bits: int = 0):
+        self.index = index
+        self._h = ctypes.c_void_p()
+        opts = index._opts("batched", MEM_HOST, MEM_DEVICE, sort, 0, False, blocks_per_sm, win_bits)
+        _check(load_library().qcp_plan_create(index._h, max_queries, max_hits, ctypes.byref(opts),
+                                              ctypes.byref(self._h)))
+
+    def run_device(self, boxes, q: int | None = None, stream: int = 0):
+        lib = load_library()
+        if isinstance(boxes, np.ndarray):
+            b = np.ascontiguousarray(boxes, dtype=np.float32).reshape(-1, 2 * self.index.dims)
+            nq, ptr, mem = b.shape[0], _ptr(b), MEM_HOST
+        else:
+            nq, ptr, mem = q, ctypes.c_void_p(_device_ptr(boxes)), MEM_DEVICE
+        total = ctypes.c_uint64()
+        offs, ids = ctypes.c_void_p(), ctypes.c_void_p()
+        _check(lib.qcp_plan_run(self._h, ptr, nq, mem, ctypes.c_void_p(stream or None), ctypes.byref(total),
+                                ctypes.byref(offs), ctypes.byref(ids)))
+        return nq, int(total.value), offs.value, ids.value
+
+    def run(self, boxes, q: int | None = None, stream: int = 0):
+        import torch
+        nq, total, offs, ids = self.run_device(boxes, q, stream)
+        o = torch.as_tensor(_DeviceArray(offs, nq + 1, "<u8"), device="cuda").cpu().numpy().copy()
+        i = (torch.as_tensor(_DeviceArray(ids, total, "<i4"), device="cuda").cpu().numpy().copy()
+             if total else np.zeros(0, np.int32))
+        return o, i
+
+    def close(self):
+        if self._h:
+            load_library().qcp_plan_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def autotune(objs, boxes, is_rect: bool = False, dims: int | None = None, key_mode: int = 0,

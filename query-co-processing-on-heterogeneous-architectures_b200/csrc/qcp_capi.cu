@@ -290,7 +290,7 @@ qcp_status ws_reserve_sort(qcp_index* ix, Workspace* ws, size_t jobs, size_t til
   return QCP_OK;
 }
 
-static void ws_destroy(Workspace* ws, qcp_index* ix) {
+void ws_destroy(Workspace* ws, qcp_index* ix) {
   cudaFree(ws->boxes);
   cudaFree(ws->items[0]);
   cudaFree(ws->items[1]);

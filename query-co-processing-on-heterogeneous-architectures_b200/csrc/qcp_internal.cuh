@@ -271,6 +271,17 @@ qcp_status run_plain(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_only,
 qcp_status init_items(Workspace* ws, uint32_t q, cudaStream_t s);
 qcp_status expand_level(qcp_index* ix, Workspace* ws, uint32_t l, int cur, cudaStream_t s);
 qcp_status write_items(qcp_index* ix, Workspace* ws, int cur, cudaStream_t s);
+// Fixed-capacity, readback-free variants for captured pipelines (qcp_plan).
+qcp_status run_batched_device(qcp_index* ix, Workspace* ws, uint32_t q, uint64_t ids_cap, bool sort,
+                              void* sort_tables, cudaStream_t s);
+qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void* tables, cudaStream_t s);
+size_t sort_tables_bytes(const qcp_index* ix, const Workspace* ws, uint32_t q);
+// Workspace construction and buffer reservation (qcp_capi.cu).
+qcp_status ws_reserve_queries(qcp_index* ix, Workspace* ws, uint32_t q);
+qcp_status ws_reserve_items(qcp_index* ix, Workspace* ws, size_t items);
+qcp_status ws_reserve_out(qcp_index* ix, Workspace* ws, size_t ids);
+qcp_status ws_reserve_sort(qcp_index* ix, Workspace* ws, size_t jobs, size_t tiles);
+void ws_destroy(Workspace* ws, qcp_index* ix);
 qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t s);
 // Sorts the slices of <= kSmallSliceCap ids; the larger slices are returned
 // as a device job list (big, *nbig entries) for the caller.

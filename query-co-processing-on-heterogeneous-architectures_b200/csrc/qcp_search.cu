@@ -316,6 +316,23 @@ __global__ void __launch_bounds__(256) k_mprs(TreeView t, const float* __restric
   }
 }
 
+// Output capacity gate of the fixed-capacity pipeline: when the batch's
+// total hits exceed the id buffer, flag it (bit 2 of *flag) and empty the
+// write pass's item list; k_gate_zero then empties every slice, so the
+// write and sort passes that follow do nothing.
+__global__ void k_gate(const unsigned long long* __restrict__ offsets, uint32_t q, unsigned long long cap,
+                       uint32_t* item_count, uint32_t* flag) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && offsets[q] > cap) {
+    atomicOr(flag, 2u);
+    *item_count = 0;
+  }
+}
+
+__global__ void k_gate_zero(unsigned long long* offsets, uint32_t q, const uint32_t* __restrict__ flag) {
+  if (!(*flag & 2u)) return;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= q; i += gridDim.x * blockDim.x) offsets[i] = 0;
+}
+
 template <int D>
 void launch_expand(uint32_t grid, cudaStream_t s, const float* boxes, const uint2* in,
                    const uint32_t* in_count, uint2* out, uint32_t* out_count, uint64_t cap,
@@ -534,6 +551,47 @@ qcp_status run_batched_counts_into(qcp_index* ix, const float* boxes, uint32_t q
     return QCP_ERR_OUTPUT_OVERFLOW;
   }
   return QCP_OK;
+}
+
+
+// The batched pipeline with fixed capacities and no host readback: the
+// frontier overflow (bit 1) and the id-capacity overflow (bit 2) are left in
+// ws->ctr[kCtrOverflow] for the caller to read after the stream has run; on
+// either, the results are incomplete.  All buffers must be reserved before
+// (ws_reserve_*, ws->out_cap >= ids_cap); sort tables as segmented_sort_device.
+// Stream-capturable.
+qcp_status run_batched_device(qcp_index* ix, Workspace* ws, uint32_t q, uint64_t ids_cap, bool sort,
+                              void* sort_tables, cudaStream_t s) {
+  const TreeView t = view_of(ix);
+  const uint32_t D = ix->dims;
+  const bool rect = ix->is_rect != 0;
+  const uint32_t grid = (uint32_t)num_sms() * ws->blocks_per_sm;
+  uint32_t* ctr = ws->ctr;
+  const uint32_t start = (ix->levels >= 2) ? ix->levels - 1 : 1;
+  QCP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * kCtrCount, s));
+  QCP_CUDA(cudaMemsetAsync(ws->qcount, 0, sizeof(uint64_t) * q, s));
+  QCP_TRY(init_items(ws, q, s));
+  int cur = 0;
+  for (uint32_t l = start; l > 1; --l) {
+    QCP_CUDA(cudaMemsetAsync(ctr + kCtrFrontier0 + (cur ^ 1), 0, sizeof(uint32_t), s));
+    QCP_TRY(expand_level(ix, ws, l, cur, s));
+    cur ^= 1;
+  }
+  QCP_DISPATCH_D(D, launch_leafscan<DD, kCount>(rect, grid, s, t, ws->boxes, ws->items[cur],
+                                                ctr + kCtrFrontier0 + cur, ctr + kCtrWork, ws->item_hits,
+                                                ws->qcount, nullptr, nullptr, nullptr, ws->items_cap,
+                                                ws->d_stats));
+  note_launch();
+  QCP_TRY(exclusive_scan_counts(ws->qcount, ws->offsets, q, ix->pool, s));
+  k_gate<<<1, 32, 0, s>>>((const unsigned long long*)ws->offsets, q, ids_cap, ctr + kCtrFrontier0 + cur,
+                          ctr + kCtrOverflow);
+  k_gate_zero<<<(q + 256) / 256, 256, 0, s>>>((unsigned long long*)ws->offsets, q, ctr + kCtrOverflow);
+  note_launch(2);
+  QCP_CUDA(cudaMemsetAsync(ws->qcursor, 0, sizeof(uint64_t) * q, s));
+  QCP_CUDA(cudaMemsetAsync(ctr + kCtrWork, 0, sizeof(uint32_t), s));
+  QCP_TRY(write_items(ix, ws, cur, s));
+  if (sort) QCP_TRY(segmented_sort_device(ix, ws, q, sort_tables, s));
+  return check_launch("batched pipeline (device counts)");
 }
 
 }  // namespace qcp

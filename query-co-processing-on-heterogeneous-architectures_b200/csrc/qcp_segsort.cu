@@ -65,8 +65,10 @@ struct BucketSmem {
   uint32_t wtot[kSmallWarps];
 };
 
-__global__ void __launch_bounds__(kSmallThreads) k_sort_small(const Job* __restrict__ jobs, uint32_t njobs,
+__global__ void __launch_bounds__(kSmallThreads) k_sort_small(const Job* __restrict__ jobs,
+                                                              const uint32_t* __restrict__ njobs_p,
                                                               int32_t* out, uint32_t idbits) {
+  const uint32_t njobs = *njobs_p;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BucketSmem& s = *reinterpret_cast<BucketSmem*>(smem_raw);
   const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
@@ -175,13 +177,17 @@ __global__ void k_classify(const unsigned long long* __restrict__ offsets, uint3
   }
 }
 
-__global__ void k_tiles_per_job(const Job* __restrict__ jobs, uint32_t njobs, uint32_t* tiles) {
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += gridDim.x * blockDim.x)
-    tiles[j] = (jobs[j].size + kTile - 1) / kTile;
+// tiles[j] for j < nmax: tiles of job j, 0 past the job count
+__global__ void k_tiles_per_job(const Job* __restrict__ jobs, const uint32_t* __restrict__ njobs_p, uint32_t nmax,
+                                uint32_t* tiles) {
+  const uint32_t njobs = *njobs_p;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nmax; j += gridDim.x * blockDim.x)
+    tiles[j] = j < njobs ? (jobs[j].size + kTile - 1) / kTile : 0u;
 }
 
 __global__ void k_tile_map(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ tile_off,
-                           uint32_t njobs, uint32_t* map) {
+                           const uint32_t* __restrict__ njobs_p, uint32_t* map) {
+  const uint32_t njobs = *njobs_p;
   for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
     const uint32_t t0 = tile_off[j], nt = tiles[j];
     for (uint32_t k = threadIdx.x; k < nt; k += blockDim.x) map[t0 + k] = j;
@@ -192,8 +198,9 @@ __global__ void k_tile_map(const uint32_t* __restrict__ tiles, const uint32_t* _
 __global__ void __launch_bounds__(kTileThreads) k_win_hist(const Job* __restrict__ jobs,
                                                            const uint32_t* __restrict__ map,
                                                            const uint32_t* __restrict__ tile_off,
-                                                           uint32_t ntiles, const int32_t* __restrict__ src,
+                                                           const uint32_t* __restrict__ ntiles_p, const int32_t* __restrict__ src,
                                                            uint32_t G, uint32_t wbits, uint32_t* whist) {
+  const uint32_t ntiles = *ntiles_p;
   extern __shared__ uint32_t h[];  // [G]
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     for (uint32_t w = threadIdx.x; w < G; w += kTileThreads) h[w] = 0;
@@ -219,10 +226,12 @@ __global__ void __launch_bounds__(kTileThreads) k_win_hist(const Job* __restrict
 }
 
 // Per job: exclusive scan over its G window counts -> bases and cursors.
-__global__ void __launch_bounds__(kTileThreads) k_win_scan(const Job* __restrict__ jobs, uint32_t njobs,
+__global__ void __launch_bounds__(kTileThreads) k_win_scan(const Job* __restrict__ jobs,
+                                                           const uint32_t* __restrict__ njobs_p,
                                                            uint32_t G, const uint32_t* __restrict__ whist,
                                                            unsigned long long* wbase,
                                                            unsigned long long* wcur) {
+  const uint32_t njobs = *njobs_p;
   __shared__ uint32_t wt[kTileWarps];
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t per = (G + kTileThreads - 1) / kTileThreads;
@@ -262,9 +271,10 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scan(const Job* __restrict
 __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restrict__ jobs,
                                                               const uint32_t* __restrict__ map,
                                                               const uint32_t* __restrict__ tile_off,
-                                                              uint32_t ntiles, const int32_t* __restrict__ src,
+                                                              const uint32_t* __restrict__ ntiles_p, const int32_t* __restrict__ src,
                                                               int32_t* __restrict__ dst, uint32_t G,
                                                               uint32_t wbits, unsigned long long* wcur) {
+  const uint32_t ntiles = *ntiles_p;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t nw = (G <= kPerWarpMaxG) ? kTileWarps : 1u;  // counter sets
   unsigned long long* gstart = reinterpret_cast<unsigned long long*>(smem_raw);  // [G]
@@ -358,11 +368,13 @@ struct RankSmem {
 //      coalesced stores, larger ranks are stored directly.
 // The ids of a window are distinct, so the ranks are a permutation of
 // [0, size) and the window comes out in ascending order.
-__global__ void __launch_bounds__(kRankThreads, 3) k_win_sort(uint32_t total, uint32_t G, uint32_t wbits,
+__global__ void __launch_bounds__(kRankThreads, 3) k_win_sort(const uint32_t* __restrict__ njobs_p, uint32_t G,
+                                                              uint32_t wbits,
                                                               const uint32_t* __restrict__ whist,
                                                               const unsigned long long* __restrict__ wbase,
                                                               const int32_t* __restrict__ src,
                                                               int32_t* __restrict__ out) {
+  const uint32_t total = *njobs_p * G;  // (job, window) pairs
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RankSmem& s = *reinterpret_cast<RankSmem*>(smem_raw);
   const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
@@ -512,8 +524,8 @@ qcp_status sort_small_slices(qcp_index* ix, Workspace* ws, uint32_t q, cudaStrea
   ws->sort_small_jobs = nsmall;
   ws->sort_msd_jobs = nbig;
   if (nsmall) {
-    k_sort_small<<<min(nsmall, sms * 3), kSmallThreads, sizeof(BucketSmem), s>>>(small, nsmall, ws->out_ids,
-                                                                                  idbits);
+    k_sort_small<<<min(nsmall, sms * 3), kSmallThreads, sizeof(BucketSmem), s>>>(small, ctr + kCtrJobs0,
+                                                                                  ws->out_ids, idbits);
     note_launch();
     QCP_TRY(check_launch("k_sort_small"));
   }
@@ -558,7 +570,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   uint32_t* tile_off = tiles + nbig;
   qcp_status st = QCP_OK;
   do {
-    k_tiles_per_job<<<(nbig + 255) / 256, 256, 0, s>>>(big, nbig, tiles);
+    k_tiles_per_job<<<(nbig + 255) / 256, 256, 0, s>>>(big, ctr + kCtrJobs1, nbig, tiles);
     note_launch();
     st = exclusive_scan<uint32_t>(tiles, tile_off, nbig, ctr + kCtrWork2, ix->pool, s);
     if (st != QCP_OK) break;
@@ -572,21 +584,20 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
     st = ws_reserve_sort(ix, ws, 0, ntiles);
     if (st != QCP_OK) break;
     uint32_t* map = ws->seg_hist;
-    k_tile_map<<<min(nbig, sms * 8), 256, 0, s>>>(tiles, tile_off, nbig, map);
+    k_tile_map<<<min(nbig, sms * 8), 256, 0, s>>>(tiles, tile_off, ctr + kCtrJobs1, map);
     if (cudaMemsetAsync(whist, 0, sizeof(uint32_t) * nw, s) != cudaSuccess) {
       st = cuda_status(cudaGetLastError(), "memset");
       break;
     }
-    k_win_hist<<<min(ntiles, sms * 8), kTileThreads, sizeof(uint32_t) * G, s>>>(big, map, tile_off, ntiles,
-                                                                                ws->out_ids, G, wbits, whist);
-    k_win_scan<<<min(nbig, sms * 16), kTileThreads, 0, s>>>(big, nbig, G, whist, wbase, wcur);
-    k_win_scatter<<<min(ntiles, sms * 6), kTileThreads, scatter_bytes, s>>>(big, map, tile_off, ntiles,
-                                                                            ws->out_ids, ws->tmp_ids, G, wbits,
-                                                                            wcur);
+    k_win_hist<<<min(ntiles, sms * 8), kTileThreads, sizeof(uint32_t) * G, s>>>(
+        big, map, tile_off, ctr + kCtrWork2, ws->out_ids, G, wbits, whist);
+    k_win_scan<<<min(nbig, sms * 16), kTileThreads, 0, s>>>(big, ctr + kCtrJobs1, G, whist, wbase, wcur);
+    k_win_scatter<<<min(ntiles, sms * 6), kTileThreads, scatter_bytes, s>>>(
+        big, map, tile_off, ctr + kCtrWork2, ws->out_ids, ws->tmp_ids, G, wbits, wcur);
     mark(ws, kEvSortPart, s);
     ws->sort_part_marked = ws->timing;
     const uint32_t grid = (uint32_t)(nw < (uint64_t)sms * 3 ? nw : (uint64_t)sms * 3);
-    k_win_sort<<<grid, kRankThreads, rank_bytes, s>>>((uint32_t)nw, G, wbits, whist, wbase, ws->tmp_ids,
+    k_win_sort<<<grid, kRankThreads, rank_bytes, s>>>(ctr + kCtrJobs1, G, wbits, whist, wbase, ws->tmp_ids,
                                                       ws->out_ids);
     note_launch(5);
     st = check_launch("segmented sort windows");
@@ -595,6 +606,71 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   } while (false);
   ix->pool.put(bytes, tables);
   return st;
+}
+
+
+// Window bits and window count of a call (ws->win_bits, bounded as in
+// segmented_sort).
+static void window_shape(const qcp_index* ix, const Workspace* ws, uint32_t* wbits, uint32_t* G) {
+  const uint32_t idbits = id_bits(ix->n);
+  uint32_t wb = ws->win_bits ? ws->win_bits : kWinBits;
+  if (wb > kWinBits) wb = kWinBits;
+  if (idbits > 13 && wb < idbits - 13) wb = idbits - 13;
+  *wbits = idbits < wb ? idbits : wb;
+  *G = 1u << (idbits - *wbits);
+}
+
+// Bytes of the per-(job, window) tables that segmented_sort_device needs for
+// q queries with ws's window bits.
+size_t sort_tables_bytes(const qcp_index* ix, const Workspace* ws, uint32_t q) {
+  uint32_t wbits = 0, G = 0;
+  window_shape(ix, ws, &wbits, &G);
+  const size_t nw = (size_t)q * G;
+  return ((nw * 4 + 15) & ~(size_t)15) + nw * 16 + (size_t)q * 8 + 64;
+}
+
+// segmented_sort without host readbacks: job and tile counts stay on the
+// device, every launch has a fixed grid and the kernels read the counts.
+// Tables (sort_tables_bytes) and the tile map (at least total/4096 + q
+// entries, ws->seg_hist) are the caller's.  Stream-capturable.
+qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void* tables, cudaStream_t s) {
+  if (q == 0) return QCP_OK;
+  const uint32_t idbits = id_bits(ix->n);
+  uint32_t wbits = 0, G = 0;
+  window_shape(ix, ws, &wbits, &G);
+  const uint32_t sms = (uint32_t)num_sms();
+  const size_t scatter_max = (size_t)(1u << (31 - kWinBits)) * 16 + kTile * 4;
+  QCP_TRY(set_sort_attrs(ix, scatter_max));
+  const uint32_t nsets = (G <= kPerWarpMaxG) ? kTileWarps : 1u;
+  const size_t scatter_bytes = (size_t)G * (8 + 4 + 4 * nsets) + kTile * 4;
+  uint32_t* ctr = ws->ctr;
+  Job* small = reinterpret_cast<Job*>(ws->jobs[0]);
+  Job* big = reinterpret_cast<Job*>(ws->jobs[1]);
+  const size_t nw = (size_t)q * G;
+  const size_t hist_bytes = (nw * 4 + 15) & ~(size_t)15;
+  uint32_t* whist = reinterpret_cast<uint32_t*>(tables);
+  unsigned long long* wbase = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(tables) + hist_bytes);
+  unsigned long long* wcur = wbase + nw;
+  uint32_t* tiles = reinterpret_cast<uint32_t*>(wcur + nw);
+  uint32_t* tile_off = tiles + q;
+  QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t) * 2, s));
+  k_classify<<<(q + 255) / 256, 256, 0, s>>>((const unsigned long long*)ws->offsets, q, small, ctr + kCtrJobs0,
+                                             big, ctr + kCtrJobs1, nullptr);
+  k_sort_small<<<sms * 3, kSmallThreads, sizeof(BucketSmem), s>>>(small, ctr + kCtrJobs0, ws->out_ids, idbits);
+  k_tiles_per_job<<<(q + 255) / 256, 256, 0, s>>>(big, ctr + kCtrJobs1, q, tiles);
+  note_launch(3);
+  QCP_TRY(exclusive_scan<uint32_t>(tiles, tile_off, q, ctr + kCtrWork2, ix->pool, s));
+  k_tile_map<<<sms * 8, 256, 0, s>>>(tiles, tile_off, ctr + kCtrJobs1, ws->seg_hist);
+  QCP_CUDA(cudaMemsetAsync(whist, 0, sizeof(uint32_t) * nw, s));
+  k_win_hist<<<sms * 8, kTileThreads, sizeof(uint32_t) * G, s>>>(big, ws->seg_hist, tile_off, ctr + kCtrWork2,
+                                                                 ws->out_ids, G, wbits, whist);
+  k_win_scan<<<sms * 16, kTileThreads, 0, s>>>(big, ctr + kCtrJobs1, G, whist, wbase, wcur);
+  k_win_scatter<<<sms * 6, kTileThreads, scatter_bytes, s>>>(big, ws->seg_hist, tile_off, ctr + kCtrWork2,
+                                                             ws->out_ids, ws->tmp_ids, G, wbits, wcur);
+  k_win_sort<<<sms * 3, kRankThreads, sizeof(RankSmem), s>>>(ctr + kCtrJobs1, G, wbits, whist, wbase,
+                                                             ws->tmp_ids, ws->out_ids);
+  note_launch(5);
+  return check_launch("segmented sort (device counts)");
 }
 
 }  // namespace qcp
