@@ -336,6 +336,50 @@ def run_ours(args, rank, world, local):
                    "output_cap_bytes": 2 << 30, "max_output_bytes": int(st["max_output_bytes"]),
                    "streams": args.serve_streams}
 
+    # ---- captured query plans (CUDA graph replay) vs qcp_query_batch ---------
+    plan_out = None
+    if args.plan_batches > 0 and world == 1 and args.workload == "gauss16m" and args.algo == "batched":
+        plan_out = {}
+        # (a) the timed batch itself through one plan
+        with qcp.Plan(ix, Q, int(stats["hits"] * 1.05) + 1024, blocks_per_sm=knobs["blocks_per_sm"],
+                      win_bits=knobs["win_bits"]) as plan:
+            plan.run_device(d_boxes, q=Q, stream=sp)
+            torch.cuda.synchronize()
+            e_a = torch.cuda.Event(enable_timing=True)
+            e_b = torch.cuda.Event(enable_timing=True)
+            e_a.record(stream)
+            for _ in range(args.steps):
+                plan.run_device(d_boxes, q=Q, stream=sp)
+            e_b.record(stream)
+            e_b.synchronize()
+            pm = e_a.elapsed_time(e_b) / args.steps
+        plan_out["batch"] = {"queries": Q, "ms_per_batch": round(pm, 4), "queries_per_s": round(Q / (pm / 1e3), 1),
+                             "direct_ms_per_batch": round(elapsed_ms / args.steps, 4)}
+        # (b) serving-sized batches: host wall time per call, both ways
+        for nb in (64, 1024):
+            need = nb * (args.plan_batches + 3)
+            _, s_boxes, _ = W.serving_stream(w.objs, rate=args.serve_rate, duration_s=1.05 * need / args.serve_rate)
+            d_sb = torch.from_numpy(np.ascontiguousarray(s_boxes[:nb * args.plan_batches])).to(dev)
+            with qcp.Plan(ix, nb, 64_000_000) as plan:
+                def direct(k):
+                    r = ix.search(d_sb[k * nb:(k + 1) * nb], q=nb, result_mem=qcp.MEM_DEVICE, stream=sp)
+                    r.release()
+
+                def planned(k):
+                    plan.run_device(d_sb[k * nb:(k + 1) * nb], q=nb, stream=sp)
+                res = {}
+                for name, fn in (("direct", direct), ("plan", planned)):
+                    for k in range(3):
+                        fn(k)
+                    lat = []
+                    for k in range(args.plan_batches):
+                        t0 = time.perf_counter()
+                        fn(k)
+                        lat.append((time.perf_counter() - t0) * 1e3)
+                    res[name + "_p50_ms"] = round(float(np.percentile(lat, 50)), 4)
+                    res[name + "_p99_ms"] = round(float(np.percentile(lat, 99)), 4)
+            plan_out[f"serving_batches_of_{nb}"] = res
+
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -403,6 +447,8 @@ def run_ours(args, rank, world, local):
     }
     if serving is not None:
         out["serving"] = serving
+    if plan_out is not None:
+        out["plan"] = plan_out
     if cpu is not None:
         out["cpu_baseline"] = cpu
     print(json.dumps(out), flush=True)
@@ -502,6 +548,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (use --fanout and defaults)")
+    ap.add_argument("--plan-batches", type=int, default=200,
+                    help="serving-sized batches timed through qcp_query_batch and a captured plan (0 = skip)")
     ap.add_argument("--serve-seconds", type=float, default=10.0,
                     help="length of the serving replay at N=1 (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=200_000.0, help="serving arrivals per second")

@@ -263,16 +263,21 @@ qcp_status qcp_plan_free(qcp_plan* plan);
 /* Serving: replays an open-loop arrival trace through continuous batching
  * over the resident index.  Request i (box i, q rows of 2*dims floats in
  * host memory) arrives arrival_s[i] seconds after the call starts
- * (non-decreasing).  `streams` worker threads, each with its own CUDA stream,
- * take every request that has arrived (up to max_batch), count their hits
- * and admit the longest prefix whose result bytes (4 per id + 8 per query)
- * fit output_cap_bytes next to the results other workers hold -- a request
- * larger than the cap runs alone -- then run it as one sorted batch; batches
- * of different workers overlap on the device.  deliver (optional) receives
- * every request's ascending ids, from the worker threads, once each.
- * latency_ms (optional, q entries) gets arrival -> results-on-host time per
- * request.  No counterpart in the reference (its Evaluator replays fixed
- * query files through Tree::Search, src/evaluator/evaluator.cpp:171-280). */
+ * (non-decreasing).  `streams` worker threads, each with its own CUDA stream
+ * and two captured query plans (qcp_plan, up to 256 and up to 4096 queries),
+ * take every request that has arrived (up to max_batch) and run it as plan
+ * replays; batches of different workers overlap on the device.  Admission by
+ * output memory: each worker's plans reserve result buffers for
+ * output_cap_bytes / streams bytes of results, so the results held at once
+ * stay under the cap; a batch whose results do not fit is split, and a
+ * single request larger than that runs alone through qcp_query_batch once
+ * its counted result bytes (4 per id + 8 per query) fit the cap next to what
+ * the other workers hold.  Plans and buffers are set up before the clock
+ * starts.  deliver (optional) receives every request's ascending ids, from
+ * the worker threads, once each.  latency_ms (optional, q entries) gets
+ * arrival -> results-on-host time per request.  No counterpart in the
+ * reference (its Evaluator replays fixed query files through Tree::Search,
+ * src/evaluator/evaluator.cpp:171-280). */
 typedef void (*qcp_deliver_fn)(void* user, uint32_t request, const int32_t* ids, uint64_t n);
 
 typedef struct qcp_serve_opts {

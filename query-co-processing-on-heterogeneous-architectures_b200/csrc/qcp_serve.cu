@@ -8,20 +8,26 @@
 //   feeder    the calling thread moves every request whose arrival time has
 //             passed into the pending queue (open loop: arrivals never wait
 //             for completions);
-//   workers   `streams` host threads, each with its own CUDA stream.  A
-//             free worker takes every pending request (up to max_batch),
-//             counts their hits (qcp_query_counts) and admits the longest
-//             prefix whose result bytes fit the output cap next to the
-//             results other workers hold (at least one request, so an
-//             oversized request still runs alone); the rest go back to the
-//             front of the queue.  The admitted batch runs through
-//             qcp_query_batch (sorted ids, copied to pinned host memory),
-//             its requests complete together, results are handed to the
-//             deliver callback and the batch's bytes are released.
+//   workers   `streams` host threads, each with its own CUDA stream and two
+//             captured query plans (qcp_plan: up to 256 and up to max_batch
+//             queries) whose result buffers are reserved before the clock
+//             starts.  A free worker takes every pending request (up to
+//             max_batch) and runs them as one plan replay; results are
+//             copied to the worker's pinned buffers, handed to the deliver
+//             callback, and the requests complete together.  A batch whose
+//             hits do not fit its plan is split in halves and replayed; a
+//             single request larger than a plan runs alone through
+//             qcp_query_batch after waiting until its result bytes fit the
+//             output cap next to what other workers hold.
 //
-// Batches on different workers overlap on the device: the library gives
-// every concurrent call its own workspace and stream.  Latency of a request
-// = time its results are on the host - its arrival time.
+// Admission by output memory: every worker's plans hold result buffers for
+// at most output_cap / streams bytes of results (ids and offsets), so the
+// results held at once never exceed the cap; requests beyond that run alone
+// under the cap as above.
+//
+// Batches on different workers overlap on the device: every worker has its
+// own plans, workspace and stream.  Latency of a request = time its results
+// are on the host - its arrival time.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -81,110 +87,204 @@ void fail(ServeState& st, qcp_status s) {
   st.mem_cv.notify_all();
 }
 
-void worker(ServeState* sp) {
-  ServeState& st = *sp;
+constexpr uint32_t kLargePlan = 4096;  // queries of a worker's larger plan
+
+struct WorkerRes {
   cudaStream_t stream = nullptr;
-  if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) {
-    fail(st, qcp::cuda_status(cudaGetLastError(), "serve stream"));
-    return;
+  qcp_plan* plans[2] = {nullptr, nullptr};  // small, large
+  uint32_t plan_q[2] = {0, 0};
+  uint64_t plan_hits = 0;
+  uint64_t* h_offs = nullptr;  // pinned, plan_q[1] + 1
+  int32_t* h_ids = nullptr;    // pinned, plan_hits
+};
+
+void free_res(WorkerRes& r) {
+  for (qcp_plan* p : r.plans)
+    if (p) qcp_plan_free(p);
+  if (r.h_offs) cudaFreeHost(r.h_offs);
+  if (r.h_ids) cudaFreeHost(r.h_ids);
+  if (r.stream) cudaStreamDestroy(r.stream);
+  r = WorkerRes();
+}
+
+// Streams, plans and pinned buffers of one worker, before the clock starts.
+qcp_status make_res(ServeState& st, WorkerRes& r) {
+  if (cudaStreamCreateWithFlags(&r.stream, cudaStreamNonBlocking) != cudaSuccess)
+    return qcp::cuda_status(cudaGetLastError(), "serve stream");
+  const uint64_t budget = st.o.output_cap_bytes / st.o.streams;  // result bytes of one worker
+  r.plan_hits = budget / 16;                                       // ids: <= budget / 4 bytes
+  if (r.plan_hits < 2) return QCP_OK;                              // no plans: every batch runs directly
+  uint64_t qmax = budget / 16 - 1;                                 // offsets: <= budget / 2 bytes
+  if (qmax > st.o.max_batch) qmax = st.o.max_batch;
+  r.plan_q[0] = qmax < 256 ? (uint32_t)qmax : 256u;
+  r.plan_q[1] = qmax < kLargePlan ? (uint32_t)qmax : kLargePlan;
+  for (int k = 0; k < 2; ++k) {
+    if (k == 1 && r.plan_q[1] == r.plan_q[0]) break;
+    qcp_status s = qcp_plan_create(st.ix, r.plan_q[k], r.plan_hits, nullptr, &r.plans[k]);
+    if (s != QCP_OK) return s;
   }
-  const uint32_t cap = st.o.max_batch;
-  std::vector<uint32_t> batch;
-  std::vector<float> boxes((size_t)cap * st.dims2);
-  std::vector<uint64_t> counts(cap);
-  for (;;) {
-    batch.clear();
-    {
-      std::unique_lock<std::mutex> lk(st.mu);
-      st.cv.wait(lk, [&] { return !st.pending.empty() || st.fed || st.error != QCP_OK; });
-      if (st.error != QCP_OK) break;
-      if (st.pending.empty()) {
-        if (st.fed) break;
-        continue;
-      }
-      while (!st.pending.empty() && batch.size() < cap) {
-        batch.push_back(st.pending.front());
-        st.pending.pop_front();
-      }
+  if (cudaHostAlloc((void**)&r.h_offs, sizeof(uint64_t) * ((size_t)r.plan_q[1] + 1), cudaHostAllocDefault) !=
+          cudaSuccess ||
+      cudaHostAlloc((void**)&r.h_ids, sizeof(int32_t) * r.plan_hits, cudaHostAllocDefault) != cudaSuccess)
+    return qcp::cuda_status(cudaGetLastError(), "serve pinned buffers");
+  return QCP_OK;
+}
+
+struct Worker {
+  ServeState& st;
+  WorkerRes& r;
+  std::vector<float> boxes;      // gathered boxes of the current batch
+  std::vector<uint32_t> batch;   // request indices of the current batch
+  std::vector<uint64_t> counts;
+
+  void account(uint32_t nb, uint64_t total, Clock::time_point now) {
+    std::lock_guard<std::mutex> g(st.mu);
+    st.done += nb;
+    st.hits += total;
+    ++st.batches;
+    st.batch_sum += nb;
+    st.last_done = now;
+  }
+
+  void finish(uint32_t first, uint32_t nb, const uint64_t* offs, const int32_t* ids, Clock::time_point now) {
+    const double t_done = since(st, now);
+    for (uint32_t k = 0; k < nb; ++k) {
+      const uint32_t req = batch[first + k];
+      if (st.latency_ms) st.latency_ms[req] = (float)((t_done - st.arrival[req]) * 1e3);
+      if (st.o.deliver) st.o.deliver(st.o.user, req, ids + (offs[k] - offs[0]), offs[k + 1] - offs[k]);
     }
-    uint32_t nb = (uint32_t)batch.size();
-    for (uint32_t k = 0; k < nb; ++k)
-      std::copy(st.boxes + (size_t)batch[k] * st.dims2, st.boxes + (size_t)(batch[k] + 1) * st.dims2,
-                boxes.begin() + (size_t)k * st.dims2);
-    qcp_query_opts qo;
-    memset(&qo, 0, sizeof(qo));
-    qo.stream = stream;
-    qcp_status s = qcp_query_counts(st.ix, boxes.data(), nb, &qo, counts.data());
+  }
+
+  void hold(uint64_t bytes, int delta) {
+    std::lock_guard<std::mutex> g(st.mem_mu);
+    if (delta > 0) {
+      st.held += bytes;
+      std::lock_guard<std::mutex> g2(st.mu);
+      st.max_held = std::max(st.max_held, st.held);
+    } else {
+      st.held -= bytes;
+    }
+  }
+
+  // requests batch[first, first + nb) through a plan; false on a failure
+  bool run_planned(uint32_t first, uint32_t nb) {
+    const uint32_t pmax = r.plans[1] ? r.plan_q[1] : r.plan_q[0];
+    if (nb > pmax) {  // larger than the largest plan: consecutive chunks
+      for (uint32_t c = 0; c < nb; c += pmax)
+        if (!run_planned(first + c, nb - c < pmax ? nb - c : pmax)) return false;
+      return true;
+    }
+    qcp_plan* plan = (nb <= r.plan_q[0]) ? r.plans[0] : r.plans[1];
+    uint64_t total = 0;
+    const uint64_t* d_offs = nullptr;
+    const int32_t* d_ids = nullptr;
+    const float* b = boxes.data() + (size_t)first * st.dims2;
+    qcp_status s = qcp_plan_run(plan, b, nb, QCP_MEM_HOST, r.stream, &total, &d_offs, &d_ids);
+    if (s == QCP_ERR_OUTPUT_OVERFLOW) {  // split and replay
+      if (nb == 1) return run_direct(first, 1);
+      const uint32_t h = nb / 2;
+      return run_planned(first, h) && run_planned(first + h, nb - h);
+    }
     if (s != QCP_OK) {
       fail(st, s);
-      break;
+      return false;
     }
-    // admission by result bytes: the longest prefix that fits the cap
-    uint64_t bytes = 8;
-    uint32_t take = 0;
-    while (take < nb) {
-      const uint64_t add = counts[take] * 4 + 8;
-      if (take > 0 && bytes + add > st.o.output_cap_bytes) break;
-      bytes += add;
-      ++take;
+    const uint64_t bytes = total * 4 + ((uint64_t)nb + 1) * 8;
+    hold(bytes, +1);
+    if (cudaMemcpyAsync(r.h_offs, d_offs, sizeof(uint64_t) * ((size_t)nb + 1), cudaMemcpyDeviceToHost, r.stream) !=
+            cudaSuccess ||
+        (total && cudaMemcpyAsync(r.h_ids, d_ids, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, r.stream) !=
+                      cudaSuccess) ||
+        cudaStreamSynchronize(r.stream) != cudaSuccess) {
+      hold(bytes, -1);
+      fail(st, qcp::cuda_status(cudaGetLastError(), "serve result copy"));
+      return false;
     }
-    if (take < nb) {
-      std::lock_guard<std::mutex> g(st.mu);
-      for (uint32_t k = nb; k-- > take;) st.pending.push_front(batch[k]);
-      st.cv.notify_all();
-      nb = take;
+    const Clock::time_point now = Clock::now();
+    finish(first, nb, r.h_offs, r.h_ids, now);
+    hold(bytes, -1);
+    st.mem_cv.notify_all();
+    account(nb, total, now);
+    return true;
+  }
+
+  // requests batch[first, first + nb) through qcp_query_batch, admitted by
+  // their counted result bytes against the output cap
+  bool run_direct(uint32_t first, uint32_t nb) {
+    qcp_query_opts qo;
+    memset(&qo, 0, sizeof(qo));
+    qo.stream = r.stream;
+    const float* b = boxes.data() + (size_t)first * st.dims2;
+    counts.resize(nb);
+    qcp_status s = qcp_query_counts(st.ix, b, nb, &qo, counts.data());
+    if (s != QCP_OK) {
+      fail(st, s);
+      return false;
     }
+    uint64_t bytes = ((uint64_t)nb + 1) * 8;
+    for (uint32_t k = 0; k < nb; ++k) bytes += counts[k] * 4;
     {
       std::unique_lock<std::mutex> lk(st.mem_mu);
       st.mem_cv.wait(lk, [&] {
         return st.failed.load() || st.held == 0 || st.held + bytes <= st.o.output_cap_bytes;
       });
-      if (st.failed.load()) break;
+      if (st.failed.load()) return false;
       st.held += bytes;
       std::lock_guard<std::mutex> g(st.mu);
       st.max_held = std::max(st.max_held, st.held);
-      ++st.inflight;
-      st.max_inflight = std::max(st.max_inflight, st.inflight);
     }
     qcp_result res;
     memset(&res, 0, sizeof(res));
-    s = qcp_query_batch(st.ix, boxes.data(), nb, &qo, &res);
+    s = qcp_query_batch(st.ix, b, nb, &qo, &res);
     const Clock::time_point now = Clock::now();
     if (s != QCP_OK) {
-      {
-        std::lock_guard<std::mutex> g(st.mem_mu);
-        st.held -= bytes;
-      }
+      hold(bytes, -1);
       fail(st, s);
-      break;
+      return false;
     }
-    const double t_done = since(st, now);
-    const uint64_t* offs = reinterpret_cast<const uint64_t*>(res.offsets);
-    const int32_t* ids = reinterpret_cast<const int32_t*>(res.ids);
-    for (uint32_t k = 0; k < nb; ++k) {
-      const uint32_t r = batch[k];
-      if (st.latency_ms) st.latency_ms[r] = (float)((t_done - st.arrival[r]) * 1e3);
-      if (st.o.deliver) st.o.deliver(st.o.user, r, ids + offs[k], offs[k + 1] - offs[k]);
-    }
+    finish(first, nb, reinterpret_cast<const uint64_t*>(res.offsets), reinterpret_cast<const int32_t*>(res.ids),
+           now);
     const uint64_t total = res.total_hits;
     qcp_result_release(&res);
-    {
-      std::lock_guard<std::mutex> g(st.mem_mu);
-      st.held -= bytes;
-    }
+    hold(bytes, -1);
     st.mem_cv.notify_all();
-    {
-      std::lock_guard<std::mutex> g(st.mu);
-      --st.inflight;
-      st.done += nb;
-      st.hits += total;
-      ++st.batches;
-      st.batch_sum += nb;
-      st.last_done = now;
+    account(nb, total, now);
+    return true;
+  }
+
+  void loop() {
+    const uint32_t cap = st.o.max_batch;
+    boxes.resize((size_t)cap * st.dims2);
+    for (;;) {
+      batch.clear();
+      {
+        std::unique_lock<std::mutex> lk(st.mu);
+        st.cv.wait(lk, [&] { return !st.pending.empty() || st.fed || st.error != QCP_OK; });
+        if (st.error != QCP_OK) break;
+        if (st.pending.empty()) {
+          if (st.fed) break;
+          continue;
+        }
+        while (!st.pending.empty() && batch.size() < cap) {
+          batch.push_back(st.pending.front());
+          st.pending.pop_front();
+        }
+        ++st.inflight;
+        st.max_inflight = std::max(st.max_inflight, st.inflight);
+      }
+      const uint32_t nb = (uint32_t)batch.size();
+      for (uint32_t k = 0; k < nb; ++k)
+        std::copy(st.boxes + (size_t)batch[k] * st.dims2, st.boxes + (size_t)(batch[k] + 1) * st.dims2,
+                  boxes.begin() + (size_t)k * st.dims2);
+      const bool ok = r.plans[0] ? run_planned(0, nb) : run_direct(0, nb);
+      {
+        std::lock_guard<std::mutex> g(st.mu);
+        --st.inflight;
+      }
+      if (!ok) break;
     }
   }
-  cudaStreamDestroy(stream);
-}
+};
 
 }  // namespace
 
@@ -214,13 +314,24 @@ extern "C" qcp_status qcp_serve_replay(qcp_index* ix, const float* boxes, const 
   if (st.o.output_cap_bytes == 0) st.o.output_cap_bytes = 2ull << 30;
   int dev = 0;
   cudaGetDevice(&dev);
+  std::vector<WorkerRes> res(st.o.streams);
+  for (auto& r : res) {
+    const qcp_status s = make_res(st, r);
+    if (s != QCP_OK) {
+      const std::string msg = qcp_last_error();
+      for (auto& x : res) free_res(x);
+      qcp::set_error(std::string("qcp_serve_replay: ") + msg);
+      return s;
+    }
+  }
   std::vector<std::thread> pool;
   st.t0 = Clock::now();
   st.last_done = st.t0;
   for (uint32_t w = 0; w < st.o.streams; ++w)
-    pool.emplace_back([&st, dev] {
+    pool.emplace_back([&st, &res, w, dev] {
       cudaSetDevice(dev);
-      worker(&st);
+      Worker wk{st, res[w], {}, {}, {}};
+      wk.loop();
     });
   // feeder: open-loop arrivals
   uint32_t next = 0;
@@ -245,6 +356,7 @@ extern "C" qcp_status qcp_serve_replay(qcp_index* ix, const float* boxes, const 
     st.cv.notify_all();
   }
   for (auto& t : pool) t.join();
+  for (auto& r : res) free_res(r);
   if (st.error != QCP_OK) {
     qcp::set_error(std::string("qcp_serve_replay: ") + st.error_msg);
     return st.error;
