@@ -380,6 +380,25 @@ def run_ours(args, rank, world, local):
                     res[name + "_p99_ms"] = round(float(np.percentile(lat, 99)), 4)
             plan_out[f"serving_batches_of_{nb}"] = res
 
+    # ---- the reference's own GPU traversal (MPHR), same data and queries ---
+    ref_gpu = None
+    if args.ref_gpu and world == 1 and not w.is_rect and w.dims == 3:
+        ref = _reference_lib(3)
+        if ref is None:
+            ref_gpu = {"unavailable": "oracle/_ref not built"}
+        else:
+            t0 = time.perf_counter()
+            h = ref.mphr_build(w.objs)
+            build_s = time.perf_counter() - t0
+            _, ms = ref.mphr_counts(h, boxes)
+            ref_gpu = {"kind": "reference MPHR kernel global_RestartScanning_and_ParentCheck "
+                               "(src/tree/mphr.cpp:303-438) built for sm_100a; batches of 128 queries, a host "
+                               "copy after each, as MPHR::Search (mphr.cpp:231-258); counts only",
+                       "value": round(Q / (ms / 1e3), 1), "unit": "queries/s", "ms_per_batch": round(ms, 3),
+                       "host_build_s": round(build_s, 2),
+                       "counts": "not compared: the kernel sums t_hit[0..255] but zeroes only [0..191] "
+                                 "(mphr.cpp:325-328), so its counts carry leftover shared memory"}
+
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -449,6 +468,8 @@ def run_ours(args, rank, world, local):
         out["serving"] = serving
     if plan_out is not None:
         out["plan"] = plan_out
+    if ref_gpu is not None:
+        out["reference_gpu"] = ref_gpu
     if cpu is not None:
         out["cpu_baseline"] = cpu
     print(json.dumps(out), flush=True)
@@ -548,6 +569,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (use --fanout and defaults)")
+    ap.add_argument("--no-ref-gpu", dest="ref_gpu", action="store_false",
+                    help="skip timing the reference's MPHR GPU kernel")
     ap.add_argument("--plan-batches", type=int, default=200,
                     help="serving-sized batches timed through qcp_query_batch and a captured plan (0 = skip)")
     ap.add_argument("--serve-seconds", type=float, default=10.0,

@@ -236,6 +236,15 @@ int ref_mphr_counts(void* h, const float* boxes, uint32_t q, uint32_t* counts, f
     uint32_t nb = (q - q0 < B) ? (q - q0) : B;
     tree::global_RestartScanning_and_ParentCheck<<<nb, GetNumberOfThreads()>>>(
         &d_query[(size_t)q0 * D2], 1, d_hit, d_root, d_node);
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {
+      fprintf(stderr, "ref_mphr_counts: kernel launch failed: %s\n", cudaGetErrorString(le));
+      cudaFree(d_query);
+      cudaFree(d_hit);
+      cudaFree(d_root);
+      cudaFree(d_node);
+      return -3;
+    }
     cudaMemcpy(counts + q0, d_hit, sizeof(ui) * nb, cudaMemcpyDeviceToHost);
   }
   cudaEventRecord(e1, 0);
