@@ -380,6 +380,25 @@ def run_ours(args, rank, world, local):
                     res[name + "_p99_ms"] = round(float(np.percentile(lat, 99)), 4)
             plan_out[f"serving_batches_of_{nb}"] = res
 
+    # ---- CPU + GPU co-processing (host walks the internal levels) ----------
+    hybrid = None
+    if args.algo == "batched" and world == 1:
+        hybrid = {"cpu_threads": os.cpu_count()}
+        levels = info["levels"]
+        for h in sorted({1, max(1, levels - 2)}):
+            ix.search(h_np, algo="hybrid", result_mem=qcp.MEM_DEVICE, stream=sp, handoff_level=h).release()
+            torch.cuda.synchronize()
+            e_a = torch.cuda.Event(enable_timing=True)
+            e_b = torch.cuda.Event(enable_timing=True)
+            e_a.record(stream)
+            for _ in range(args.steps):
+                ix.search(h_np, algo="hybrid", result_mem=qcp.MEM_DEVICE, stream=sp, handoff_level=h,
+                          blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"]).release()
+            e_b.record(stream)
+            e_b.synchronize()
+            hm = e_a.elapsed_time(e_b) / args.steps
+            hybrid[f"handoff_level_{h}"] = {"queries_per_s": round(Q / (hm / 1e3), 1), "ms_per_batch": round(hm, 3)}
+
     # ---- the reference's own GPU traversal (MPHR), same data and queries ---
     ref_gpu = None
     if args.ref_gpu and world == 1 and not w.is_rect and w.dims == 3:
@@ -470,6 +489,8 @@ def run_ours(args, rank, world, local):
         out["plan"] = plan_out
     if ref_gpu is not None:
         out["reference_gpu"] = ref_gpu
+    if hybrid is not None:
+        out["hybrid"] = hybrid
     if cpu is not None:
         out["cpu_baseline"] = cpu
     print(json.dumps(out), flush=True)

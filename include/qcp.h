@@ -95,7 +95,13 @@ typedef enum qcp_algo {
   QCP_ALGO_BATCHED = 0,
   /* One query per CUDA block, restart-scanning + parent-check traversal
    * (the reference's MPRS, src/tree/mphr.cpp:303-438), emitting ids. */
-  QCP_ALGO_PLAIN = 1
+  QCP_ALGO_PLAIN = 1,
+  /* CPU + GPU co-processing (the reference's Hybrid tree,
+   * src/tree/hybrid.cpp:451-760): host threads walk the internal levels of
+   * every query down to opts->handoff_level and hand the (query, node) items
+   * of that level to the GPU, which expands the rest and scans the leaves,
+   * writes and sorts as QCP_ALGO_BATCHED does. */
+  QCP_ALGO_HYBRID = 2
 } qcp_algo;
 
 typedef struct qcp_query_opts {
@@ -111,7 +117,11 @@ typedef struct qcp_query_opts {
    * 12; raised where the id range would need more than 8192 windows). */
   uint32_t blocks_per_sm;
   uint32_t win_bits;
-  uint32_t reserved_;
+  /* QCP_ALGO_HYBRID: host threads of the upper-tree walk (0 = all cores) and
+   * the tree level whose items go to the GPU (0 or 1 = the leaves' parents;
+   * the root's level = everything on the GPU). */
+  uint32_t cpu_threads;
+  uint32_t handoff_level;
 } qcp_query_opts;
 
 /* flags: record CUDA events around every phase of the call; the times are

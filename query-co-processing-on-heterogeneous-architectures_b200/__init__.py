@@ -28,7 +28,7 @@ STATUS_NAMES = {
 }
 MEM_HOST, MEM_DEVICE = 0, 1
 KEY_NORM, KEY_REF = 0, 1
-ALGO_BATCHED, ALGO_PLAIN = 0, 1
+ALGO_BATCHED, ALGO_PLAIN, ALGO_HYBRID = 0, 1, 2
 
 
 class QcpError(RuntimeError):
@@ -56,7 +56,7 @@ class QueryOpts(ctypes.Structure):
                 ("result_mem", ctypes.c_uint32), ("unsorted", ctypes.c_uint32),
                 ("stream", ctypes.c_void_p), ("flags", ctypes.c_uint32),
                 ("blocks_per_sm", ctypes.c_uint32), ("win_bits", ctypes.c_uint32),
-                ("reserved_", ctypes.c_uint32)]
+                ("cpu_threads", ctypes.c_uint32), ("handoff_level", ctypes.c_uint32)]
 
 
 QUERY_TIMING = 1
@@ -293,14 +293,16 @@ class Index:
         return keys, ids, mbr
 
     # -- queries --------------------------------------------------------------
-    def _opts(self, algo, boxes_mem, result_mem, sort, stream, timing=False, blocks_per_sm=0, win_bits=0):
-        a = {"batched": ALGO_BATCHED, "plain": ALGO_PLAIN}.get(algo, algo)
+    def _opts(self, algo, boxes_mem, result_mem, sort, stream, timing=False, blocks_per_sm=0, win_bits=0,
+              cpu_threads=0, handoff_level=0):
+        a = {"batched": ALGO_BATCHED, "plain": ALGO_PLAIN, "hybrid": ALGO_HYBRID}.get(algo, algo)
         return QueryOpts(a, boxes_mem, result_mem, 0 if sort else 1, ctypes.c_void_p(stream or None),
-                         QUERY_TIMING if timing else 0, blocks_per_sm, win_bits, 0)
+                         QUERY_TIMING if timing else 0, blocks_per_sm, win_bits, cpu_threads, handoff_level)
 
     def search(self, boxes, algo="batched", sort: bool = True, result_mem: int = MEM_HOST,
                q: int | None = None, stream: int = 0, timing: bool = False,
-               copy: bool = True, blocks_per_sm: int = 0, win_bits: int = 0) -> SearchResult:
+               copy: bool = True, blocks_per_sm: int = 0, win_bits: int = 0, cpu_threads: int = 0,
+               handoff_level: int = 0) -> SearchResult:
         """Run a batch of box queries.  Host numpy boxes (q x 2D) or a CUDA
         tensor/pointer (then pass q).  Host results are copied into numpy
         arrays (copy=False: numpy views of the library's pinned result arena,
@@ -314,7 +316,8 @@ class Index:
             if q is None:
                 raise ValueError("device boxes need q")
             b, nq, ptr, bmem = boxes, q, ctypes.c_void_p(_device_ptr(boxes)), MEM_DEVICE
-        opts = self._opts(algo, bmem, result_mem, sort, stream, timing, blocks_per_sm, win_bits)
+        opts = self._opts(algo, bmem, result_mem, sort, stream, timing, blocks_per_sm, win_bits, cpu_threads,
+                          handoff_level)
         r = Result()
         _check(lib.qcp_query_batch(self._h, ptr, nq, ctypes.byref(opts), ctypes.byref(r)))
         if result_mem == MEM_HOST and not copy:

@@ -522,7 +522,7 @@ static qcp_status run_query(qcp_index* ix, const float* boxes, uint32_t q, const
     set_error("index and boxes must be non-NULL");
     return QCP_ERR_BAD_ARG;
   }
-  if (o.algo > QCP_ALGO_PLAIN || o.boxes_mem > QCP_MEM_DEVICE || o.result_mem > QCP_MEM_DEVICE) {
+  if (o.algo > QCP_ALGO_HYBRID || o.boxes_mem > QCP_MEM_DEVICE || o.result_mem > QCP_MEM_DEVICE) {
     set_error("invalid query options");
     return QCP_ERR_BAD_ARG;
   }
@@ -540,6 +540,23 @@ static qcp_status run_query(qcp_index* ix, const float* boxes, uint32_t q, const
   ws->blocks_per_sm = o.blocks_per_sm ? (o.blocks_per_sm > 32 ? 32u : o.blocks_per_sm) : 8u;
   ws->win_bits = o.win_bits ? (o.win_bits < 12 ? 12u : o.win_bits) : 18u;
   ws->sort_small_jobs = ws->sort_msd_jobs = 0;
+  ws->hybrid = o.algo == QCP_ALGO_HYBRID;
+  ws->cpu_threads = o.cpu_threads;
+  ws->handoff_level = o.handoff_level ? o.handoff_level : 1u;
+  ws->h_boxes = nullptr;
+  if (st == QCP_OK && q && ws->hybrid) {
+    // the host walk reads the boxes on the host
+    if (o.boxes_mem == QCP_MEM_HOST) {
+      ws->h_boxes = boxes;
+    } else {
+      ws->h_boxes_copy.resize(2 * (size_t)ix->dims * q);
+      if (cudaMemcpyAsync(ws->h_boxes_copy.data(), boxes, sizeof(float) * ws->h_boxes_copy.size(),
+                          cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess)
+        st = cuda_status(cudaGetLastError(), "copy query boxes to the host");
+      ws->h_boxes = ws->h_boxes_copy.data();
+    }
+  }
   if (st == QCP_OK && q) {
     const size_t bytes = sizeof(float) * 2 * ix->dims * (size_t)q;
     cudaError_t e = cudaMemcpyAsync(ws->boxes, boxes, bytes,

@@ -108,6 +108,13 @@ struct Workspace {
   bool sort_part_marked = false;
   uint32_t blocks_per_sm = 8;    // traversal grid = SMs x this, this call
   uint32_t win_bits = 18;        // sort window, this call
+  // CPU + GPU co-processing (QCP_ALGO_HYBRID) of this call
+  bool hybrid = false;
+  uint32_t cpu_threads = 0, handoff_level = 1;
+  const float* h_boxes = nullptr;    // the call's boxes in host memory
+  std::vector<float> h_boxes_copy;   // when the caller's boxes are on the device
+  std::vector<uint2> h_items;        // host-walked frontier
+  uint32_t h_nitems = 0;
   uint32_t sort_small_jobs = 0, sort_msd_jobs = 0;
 };
 
@@ -155,6 +162,11 @@ struct qcp_index {
   int32_t* ids = nullptr;             // [npad] input id of each sorted position
   uint64_t* keys = nullptr;           // [n] sorted keys
   float* mbr[qcp::kMaxLevels] = {nullptr};  // per level [2*dims][level_pad]
+  // host copies of the internal levels' MBRs (levels >= 1), made on the first
+  // CPU + GPU co-processing query
+  std::mutex host_mbr_mu;
+  std::vector<float> host_mbr[qcp::kMaxLevels];
+  bool host_mbr_ready = false;
   uint64_t device_bytes = 0;
 
   qcp::DevPool pool;
@@ -171,13 +183,13 @@ namespace qcp {
 
 // Overlap of a query box with an entry [lo, hi] in every dimension:
 // !(q.lo > e.hi || q.hi < e.lo), the predicate of src/node/node_soa.cpp:94-113.
-__device__ __forceinline__ bool overlaps1(float qlo, float qhi, float lo, float hi) {
+__host__ __device__ __forceinline__ bool overlaps1(float qlo, float qhi, float lo, float hi) {
   return !(qlo > hi || qhi < lo);
 }
 // Entry [lo, hi] lies inside the query box in one dimension.  Only used to
 // skip the per-entry test of leaves whose MBR is covered by the query: every
 // finite entry inside such an MBR passes overlaps1.
-__device__ __forceinline__ bool inside1(float qlo, float qhi, float lo, float hi) {
+__host__ __device__ __forceinline__ bool inside1(float qlo, float qhi, float lo, float hi) {
   return qlo <= lo && hi <= qhi;
 }
 
@@ -271,6 +283,9 @@ qcp_status run_plain(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_only,
 qcp_status init_items(Workspace* ws, uint32_t q, cudaStream_t s);
 qcp_status expand_level(qcp_index* ix, Workspace* ws, uint32_t l, int cur, cudaStream_t s);
 qcp_status write_items(qcp_index* ix, Workspace* ws, int cur, cudaStream_t s);
+// Host walk of the internal levels for QCP_ALGO_HYBRID: the (query, node)
+// items of `level` for every query into items[0] and its counter.
+qcp_status host_frontier(qcp_index* ix, Workspace* ws, uint32_t q, uint32_t level, cudaStream_t s);
 // Fixed-capacity, readback-free variants for captured pipelines (qcp_plan).
 qcp_status run_batched_device(qcp_index* ix, Workspace* ws, uint32_t q, uint64_t ids_cap, bool sort,
                               void* sort_tables, cudaStream_t s);

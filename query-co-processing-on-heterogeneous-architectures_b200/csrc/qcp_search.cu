@@ -23,7 +23,9 @@
 //
 // The hit predicate everywhere is the reference's closed-interval test
 // (src/node/node_soa.cpp:94-113).
+#include <algorithm>
 #include <cfloat>
+#include <thread>
 
 #include "qcp_internal.cuh"
 #include "qcp_tree.cuh"
@@ -424,11 +426,21 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
     QCP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * kCtrCount, s));
     QCP_CUDA(cudaMemsetAsync(ws->d_stats, 0, sizeof(unsigned long long) * kStatCount, s));
     QCP_CUDA(cudaMemsetAsync(ws->qcount, 0, sizeof(uint64_t) * q, s));
-    QCP_TRY(init_items(ws, q, s));
-    QCP_CUDA(cudaMemcpyAsync(ws->d_stats + kStatLevel0 + start, ctr + kCtrFrontier0, sizeof(uint32_t),
+    // the GPU's first level: the root's, or the hand-off level of a CPU + GPU
+    // co-processing call whose host threads walked the levels above
+    uint32_t gpu_start = start;
+    if (ws->hybrid) {
+      gpu_start = ws->handoff_level < 1 ? 1u : (ws->handoff_level > start ? start : ws->handoff_level);
+    }
+    if (gpu_start < start) {
+      QCP_TRY(host_frontier(ix, ws, q, gpu_start, s));
+    } else {
+      QCP_TRY(init_items(ws, q, s));
+    }
+    QCP_CUDA(cudaMemcpyAsync(ws->d_stats + kStatLevel0 + gpu_start, ctr + kCtrFrontier0, sizeof(uint32_t),
                              cudaMemcpyDeviceToDevice, s));
     int cur = 0;
-    for (uint32_t l = start; l > 1; --l) {
+    for (uint32_t l = gpu_start; l > 1; --l) {
       const int nxt = cur ^ 1;
       QCP_CUDA(cudaMemsetAsync(ctr + kCtrFrontier0 + nxt, 0, sizeof(uint32_t), s));
       QCP_TRY(expand_level(ix, ws, l, cur, s));
@@ -592,6 +604,94 @@ qcp_status run_batched_device(qcp_index* ix, Workspace* ws, uint32_t q, uint64_t
   QCP_TRY(write_items(ix, ws, cur, s));
   if (sort) QCP_TRY(segmented_sort_device(ix, ws, q, sort_tables, s));
   return check_launch("batched pipeline (device counts)");
+}
+
+
+// ---------------------------------------------------------------------------
+// CPU + GPU co-processing: the host walks the internal levels.
+//
+// The reference's Hybrid::Search (src/tree/hybrid.cpp:451-760) gives every
+// host thread a share of the queries; per query the thread walks the upper
+// tree (Hybrid::TraverseInternalNodes, :801-960) to a run of leaf nodes and
+// launches a GPU scan of that run, one launch per run.  Here the host threads
+// walk every query of the batch down to the hand-off level at once and the
+// GPU gets the whole frontier in one copy; expansion below the hand-off
+// level, the leaf scan, the write and the sort stay on the GPU.  The host
+// uses a copy of the internal levels' MBRs and the same closed-interval
+// predicate as the kernels.
+// ---------------------------------------------------------------------------
+static qcp_status ensure_host_mbr(qcp_index* ix) {
+  std::lock_guard<std::mutex> g(ix->host_mbr_mu);
+  if (ix->host_mbr_ready) return QCP_OK;
+  for (uint32_t l = 1; l < ix->levels; ++l) {
+    const size_t n = 2 * (size_t)ix->dims * ix->level_pad[l];
+    ix->host_mbr[l].resize(n);
+    QCP_CUDA(cudaMemcpy(ix->host_mbr[l].data(), ix->mbr[l], sizeof(float) * n, cudaMemcpyDeviceToHost));
+  }
+  ix->host_mbr_ready = true;
+  return QCP_OK;
+}
+
+qcp_status host_frontier(qcp_index* ix, Workspace* ws, uint32_t q, uint32_t level, cudaStream_t s) {
+  QCP_TRY(ensure_host_mbr(ix));
+  const uint32_t D = ix->dims, F = ix->fanout, top = ix->levels - 1;
+  const float* boxes = ws->h_boxes;
+  uint32_t T = ws->cpu_threads ? ws->cpu_threads : std::thread::hardware_concurrency();
+  if (T == 0) T = 1;
+  if (T > 64) T = 64;
+  if (T > q) T = q ? q : 1;
+  std::vector<std::vector<uint2>> part(T);
+  auto walk = [&](uint32_t t) {
+    const uint32_t q0 = (uint32_t)((uint64_t)q * t / T), q1 = (uint32_t)((uint64_t)q * (t + 1) / T);
+    std::vector<std::pair<uint32_t, uint64_t>> stack;  // (level, node)
+    auto& out = part[t];
+    for (uint32_t qq = q0; qq < q1; ++qq) {
+      const float* b = boxes + (size_t)qq * 2 * D;
+      stack.clear();
+      stack.emplace_back(top, 0);
+      while (!stack.empty()) {
+        const uint32_t l = stack.back().first;
+        const uint64_t node = stack.back().second;
+        stack.pop_back();
+        const uint32_t cl = l - 1;
+        const float* m = ix->host_mbr[cl].data();
+        const uint64_t pad = ix->level_pad[cl];
+        const uint64_t c0 = node * F;
+        const uint64_t c1 = std::min<uint64_t>(c0 + F, ix->level_nodes[cl]);
+        // children in reverse so that the stack pops them in order
+        for (uint64_t c = c1; c-- > c0;) {
+          bool ov = true;
+          for (uint32_t d = 0; d < D && ov; ++d) ov = overlaps1(b[d], b[D + d], m[d * pad + c], m[(D + d) * pad + c]);
+          if (!ov) continue;
+          if (cl == level) out.push_back(make_uint2(qq, (uint32_t)c));
+          else stack.emplace_back(cl, c);
+        }
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (uint32_t t = 1; t < T; ++t) pool.emplace_back(walk, t);
+  walk(0);
+  for (auto& th : pool) th.join();
+  size_t n = 0;
+  for (auto& p : part) n += p.size();
+  ws->h_items.resize(n ? n : 1);
+  size_t k = 0;
+  for (auto& p : part) {
+    std::copy(p.begin(), p.end(), ws->h_items.begin() + k);
+    k += p.size();
+  }
+  if (n > 0xffffffffull) {
+    set_error("co-processing frontier exceeds 2^32 items");
+    return QCP_ERR_OOM;
+  }
+  QCP_TRY(ws_reserve_items(ix, ws, n));
+  ws->h_nitems = (uint32_t)n;
+  if (n) QCP_CUDA(cudaMemcpyAsync(ws->items[0], ws->h_items.data(), sizeof(uint2) * n, cudaMemcpyHostToDevice, s));
+  QCP_CUDA(cudaMemcpyAsync(ws->ctr + kCtrFrontier0, &ws->h_nitems, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  // pageable sources: wait for the copies before the host vectors change
+  QCP_CUDA(cudaStreamSynchronize(s));
+  return QCP_OK;
 }
 
 }  // namespace qcp
