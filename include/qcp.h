@@ -62,7 +62,15 @@ typedef enum qcp_key_mode {
   /* The reference's key: (long long)(1e6f * p) with 20 bits per dimension
    * for D > 2 and 31 for D == 2 (src/tree/tree.cpp:597,
    * src/mapper/hilbert_mapper.cpp:21-23).  Defined for D*bits <= 64. */
-  QCP_KEY_REF = 1
+  QCP_KEY_REF = 1,
+  /* k-means-clustered keys (the reference's CLUSTER_TYPE_KMEANSHILBERT,
+   * src/mapper/kmeans_mapper.cpp:204-259), cluster-major: the objects are
+   * clustered by k-means (kmeans_clusters centres, at most kmeans_iters
+   * assignments), the clusters are ranked by the QCP_KEY_NORM key of their
+   * centres, and an object's 64-bit key is its cluster's rank in the top
+   * ceil(log2 K) bits followed by its own QCP_KEY_NORM key.  Deterministic:
+   * centres start at the objects floor(k*n/K), sums are exact fixed point. */
+  QCP_KEY_KMEANS = 2
 } qcp_key_mode;
 
 typedef struct qcp_build_opts {
@@ -71,6 +79,8 @@ typedef struct qcp_build_opts {
   uint32_t key_bits;  /* bits per dimension; 0 = the mode's default */
   uint32_t input_mem; /* qcp_mem of objs */
   void* stream;       /* cudaStream_t for the build; NULL = legacy default stream */
+  uint32_t kmeans_clusters; /* QCP_KEY_KMEANS: centres; 0 = min(1024, n) (the reference uses 20000) */
+  uint32_t kmeans_iters;    /* QCP_KEY_KMEANS: most assignments; 0 = 30 (the reference: 1000) */
 } qcp_build_opts;
 
 typedef struct qcp_index qcp_index; /* opaque, device resident */

@@ -82,6 +82,61 @@ class Oracle:
         self.lib.oracle_sort_perm(_p(k), k.shape[0], _p(out))
         return out
 
+    def kmeans_keys(self, objs, dims, is_rect, bits, clusters, iters):
+        """Restatement of the library's k-means-clustered keys (QCP_KEY_KMEANS),
+        in numpy + the C key above: representative point (the object, or the
+        FP32 centre 0.5*(lo+hi) of a rectangle); centres start at the objects
+        floor(k*n/K); assignment = FP32 squared distance accumulated dimension
+        by dimension, first minimum; update = mean through 64-bit fixed point
+        relative to the bounding box (32 fractional bits); stop when at most
+        1e-5 of the objects changed or after `iters` assignments; clusters
+        ranked by the normalised key of their centre (ties by index); key =
+        rank in the top ceil(log2 K) bits, the object's own normalised key
+        below.  The reference's clustering step this follows is
+        KmeansMapper::ClusteringBranches (src/mapper/kmeans_mapper.cpp:204-259)
+        with cuda_kmeans (:15-199)."""
+        o = self._objs(objs)
+        n = o.shape[0]
+        rep = (np.float32(0.5) * (o[:, :dims] + o[:, dims:2 * dims])).astype(np.float32) if is_rect else o[:, :dims]
+        K = max(1, min(int(clusters), n))
+        lo = rep.min(0).astype(np.float64)
+        hi = rep.max(0).astype(np.float64)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            scale = np.where((hi > lo) & np.isfinite(hi - lo), 4294967296.0 / (hi - lo), 0.0)
+        cen = rep[(np.arange(K, dtype=np.uint64) * np.uint64(n)) // np.uint64(K)].copy()
+        member = np.full(n, -1, np.int64)
+        f = (rep.astype(np.float64) - lo) * scale
+        f[~(f > 0)] = 0.0
+        f = np.minimum(f, 4294967296.0).astype(np.uint64)
+        for _ in range(int(iters)):
+            dist = np.zeros((n, K), np.float32)
+            for d in range(dims):
+                t = rep[:, d, None] - cen[None, :, d]
+                dist = dist + t * t
+            arg = dist.argmin(1)
+            changes = int((arg != member).sum())
+            member = arg
+            cnt = np.bincount(arg, minlength=K).astype(np.uint64)
+            for d in range(dims):
+                sums = np.zeros(K, np.uint64)
+                np.add.at(sums, arg, f[:, d])
+                upd = (cnt > 0) & (scale[d] > 0)
+                cen[upd, d] = (lo[d] + (sums[upd].astype(np.float64) / cnt[upd].astype(np.float64)) / scale[d]
+                               ).astype(np.float32)
+            if changes / n <= 1e-5:
+                break
+        ckey = self.hilbert_keys(cen, dims, False, bits, 1)
+        order = np.lexsort((np.arange(K), ckey))
+        rank = np.empty(K, np.uint64)
+        rank[order] = np.arange(K, dtype=np.uint64)
+        rbits = 1
+        while rbits < 32 and (1 << rbits) < K:
+            rbits += 1
+        own = self.hilbert_keys(o, dims, is_rect, bits, 1)
+        own_bits = dims * bits
+        shift = own_bits - (64 - rbits) if own_bits > 64 - rbits else 0
+        return (rank[member] << np.uint64(64 - rbits)) | (own >> np.uint64(shift))
+
     def level_sizes(self, n, fanout):
         out = np.zeros(64, np.uint64)
         L = self.lib.oracle_level_sizes(n, fanout, _p(out), 64)

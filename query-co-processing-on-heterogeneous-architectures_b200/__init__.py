@@ -27,7 +27,7 @@ STATUS_NAMES = {
     4: "QCP_ERR_TIMEOUT", 5: "QCP_ERR_CUDA", 6: "QCP_ERR_NO_DEVICE", 7: "QCP_ERR_IO",
 }
 MEM_HOST, MEM_DEVICE = 0, 1
-KEY_NORM, KEY_REF = 0, 1
+KEY_NORM, KEY_REF, KEY_KMEANS = 0, 1, 2
 ALGO_BATCHED, ALGO_PLAIN, ALGO_HYBRID = 0, 1, 2
 
 
@@ -41,7 +41,8 @@ class QcpError(RuntimeError):
 class BuildOpts(ctypes.Structure):
     _fields_ = [("fanout", ctypes.c_uint32), ("key_mode", ctypes.c_uint32),
                 ("key_bits", ctypes.c_uint32), ("input_mem", ctypes.c_uint32),
-                ("stream", ctypes.c_void_p)]
+                ("stream", ctypes.c_void_p), ("kmeans_clusters", ctypes.c_uint32),
+                ("kmeans_iters", ctypes.c_uint32)]
 
 
 class IndexInfo(ctypes.Structure):
@@ -212,11 +213,12 @@ class Index:
     @classmethod
     def build(cls, objs, dims: int | None = None, is_rect: bool = False, fanout: int = 128,
               key_mode: int = KEY_NORM, key_bits: int = 0, n: int | None = None,
-              stream: int = 0) -> "Index":
+              stream: int = 0, kmeans_clusters: int = 0, kmeans_iters: int = 0) -> "Index":
         """Build from a host numpy array (n x D points or n x 2D rects) or a
         CUDA tensor / device pointer (then pass n and dims)."""
         lib = load_library()
-        opts = BuildOpts(fanout, key_mode, key_bits, MEM_HOST, ctypes.c_void_p(stream or None))
+        opts = BuildOpts(fanout, key_mode, key_bits, MEM_HOST, ctypes.c_void_p(stream or None), kmeans_clusters,
+                         kmeans_iters)
         if isinstance(objs, np.ndarray):
             a = np.ascontiguousarray(objs, dtype=np.float32)
             n = a.shape[0]

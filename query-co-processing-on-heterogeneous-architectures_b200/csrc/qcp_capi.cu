@@ -415,11 +415,12 @@ static qcp_status build_impl(const float* objs, uint64_t n, uint32_t dims, uint3
     set_error("fanout must be a multiple of 32 in [32, 256]");
     return QCP_ERR_BAD_ARG;
   }
-  if (o.key_mode > QCP_KEY_REF || o.input_mem > QCP_MEM_DEVICE) {
+  if (o.key_mode > QCP_KEY_KMEANS || o.input_mem > QCP_MEM_DEVICE) {
     set_error("invalid key_mode or input_mem");
     return QCP_ERR_BAD_ARG;
   }
-  const uint32_t bits = o.key_bits ? o.key_bits : default_bits(o.key_mode, dims);
+  const uint32_t bits =
+      o.key_bits ? o.key_bits : default_bits(o.key_mode == QCP_KEY_KMEANS ? QCP_KEY_NORM : o.key_mode, dims);
   if (bits > 32 || (uint64_t)bits * dims > 64) {
     set_error("key bits per dimension must be <= 32 and dims*bits <= 64");
     return QCP_ERR_BAD_ARG;
@@ -467,11 +468,17 @@ static qcp_status build_impl(const float* objs, uint64_t n, uint32_t dims, uint3
     st = cuda_status(cudaGetLastError(), "memset");
     goto fail;
   }
-  if ((st = build_keys((const float*)d_objs, n, dims, is_rect, ix->key_mode, bits, ix->keys,
-                       (uint32_t*)vals, s)) != QCP_OK)
+  if (ix->key_mode == QCP_KEY_KMEANS) {
+    const uint32_t K = o.kmeans_clusters ? o.kmeans_clusters : (uint32_t)(n < 1024 ? n : 1024);
+    if ((st = build_keys_kmeans((const float*)d_objs, n, dims, is_rect, bits, K,
+                                o.kmeans_iters ? o.kmeans_iters : 30u, ix->keys, (uint32_t*)vals, s)) != QCP_OK)
+      goto fail;
+  } else if ((st = build_keys((const float*)d_objs, n, dims, is_rect, ix->key_mode, bits, ix->keys,
+                              (uint32_t*)vals, s)) != QCP_OK) {
     goto fail;
+  }
   if ((st = radix_sort_pairs(ix->keys, (uint32_t*)vals, (uint64_t*)keys_tmp, (uint32_t*)vals_tmp, n,
-                             dims * bits, ix->pool, s, &in_tmp)) != QCP_OK)
+                             ix->key_mode == QCP_KEY_KMEANS ? 64u : dims * bits, ix->pool, s, &in_tmp)) != QCP_OK)
     goto fail;
   if (in_tmp) {
     if (cudaMemcpyAsync(ix->keys, keys_tmp, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, s) !=

@@ -267,6 +267,9 @@ qcp_status build_keys(const float* objs, uint64_t n, uint32_t dims, uint32_t is_
 qcp_status radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp,
                             uint64_t n, uint32_t key_bits, DevPool& pool, cudaStream_t s,
                             bool* result_in_tmp);
+qcp_status build_keys_kmeans(const float* objs, uint64_t n, uint32_t dims, uint32_t is_rect, uint32_t bits,
+                             uint32_t K, uint32_t max_iters, uint64_t* keys, uint32_t* vals, cudaStream_t s);
+uint32_t kmeans_rank_bits(uint32_t K);
 qcp_status build_pack(qcp_index* ix, const float* objs, const uint32_t* perm, cudaStream_t s,
                       uint32_t* d_bad);
 qcp_status build_levels(qcp_index* ix, cudaStream_t s);
