@@ -151,7 +151,17 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
           if (e1 > t.n) e1 = t.n;
           const int32_t* src = t.ids + e0;
           const uint64_t cnt = e1 - e0;
-          for (uint64_t j = lane; j < cnt; j += 32) out[wpos + j] = __ldg(src + j);
+          // four loads in flight per lane before their stores
+          uint64_t j = lane;
+          for (; j + 96 < cnt; j += 128) {
+            const int32_t a = __ldg(src + j), b = __ldg(src + j + 32);
+            const int32_t c = __ldg(src + j + 64), d = __ldg(src + j + 96);
+            out[wpos + j] = a;
+            out[wpos + j + 32] = b;
+            out[wpos + j + 64] = c;
+            out[wpos + j + 96] = d;
+          }
+          for (; j < cnt; j += 32) out[wpos + j] = __ldg(src + j);
           wpos += cnt;
         }
       }

@@ -478,6 +478,19 @@ __global__ void __launch_bounds__(kRankThreads, 3) k_win_sort(const uint32_t* __
 
 qcp_status ws_reserve_sort(qcp_index* ix, Workspace* ws, size_t jobs, size_t tiles);
 
+// Blocks of k_win_scatter resident per SM with `smem` bytes of dynamic shared
+// memory (its registers, not its shared memory, are the usual limit): the
+// persistent grid is this many blocks per SM, so that no block waits for a
+// second wave.
+static uint32_t scatter_blocks_per_sm(size_t smem) {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_win_scatter, kTileThreads, smem) != cudaSuccess || b < 1) {
+    cudaGetLastError();
+    b = 1;
+  }
+  return (uint32_t)b;
+}
+
 static uint32_t id_bits(uint64_t n) {
   uint32_t idbits = 1;
   while (idbits < 31 && (1ull << idbits) < n) ++idbits;
@@ -592,7 +605,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
     k_win_hist<<<min(ntiles, sms * 8), kTileThreads, sizeof(uint32_t) * G, s>>>(
         big, map, tile_off, ctr + kCtrWork2, ws->out_ids, G, wbits, whist);
     k_win_scan<<<min(nbig, sms * 16), kTileThreads, 0, s>>>(big, ctr + kCtrJobs1, G, whist, wbase, wcur);
-    k_win_scatter<<<min(ntiles, sms * 6), kTileThreads, scatter_bytes, s>>>(
+    k_win_scatter<<<min(ntiles, sms * scatter_blocks_per_sm(scatter_bytes)), kTileThreads, scatter_bytes, s>>>(
         big, map, tile_off, ctr + kCtrWork2, ws->out_ids, ws->tmp_ids, G, wbits, wcur);
     mark(ws, kEvSortPart, s);
     ws->sort_part_marked = ws->timing;
@@ -665,7 +678,8 @@ qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void*
   k_win_hist<<<sms * 8, kTileThreads, sizeof(uint32_t) * G, s>>>(big, ws->seg_hist, tile_off, ctr + kCtrWork2,
                                                                  ws->out_ids, G, wbits, whist);
   k_win_scan<<<sms * 16, kTileThreads, 0, s>>>(big, ctr + kCtrJobs1, G, whist, wbase, wcur);
-  k_win_scatter<<<sms * 6, kTileThreads, scatter_bytes, s>>>(big, ws->seg_hist, tile_off, ctr + kCtrWork2,
+  k_win_scatter<<<sms * scatter_blocks_per_sm(scatter_bytes), kTileThreads, scatter_bytes, s>>>(
+      big, ws->seg_hist, tile_off, ctr + kCtrWork2,
                                                              ws->out_ids, ws->tmp_ids, G, wbits, wcur);
   k_win_sort<<<sms * 3, kRankThreads, sizeof(RankSmem), s>>>(ctr + kCtrJobs1, G, wbits, whist, wbase,
                                                              ws->tmp_ids, ws->out_ids);
