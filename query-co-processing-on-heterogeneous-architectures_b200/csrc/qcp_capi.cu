@@ -290,7 +290,15 @@ qcp_status ws_reserve_sort(qcp_index* ix, Workspace* ws, size_t jobs, size_t til
   return QCP_OK;
 }
 
+qcp_status ws_reserve_qwhist(Workspace* ws, size_t n) {
+  size_t cap = ws->qwhist_cap;
+  QCP_TRY(grow(&ws->qwhist, &cap, n, 4096));
+  ws->qwhist_cap = cap;
+  return QCP_OK;
+}
+
 void ws_destroy(Workspace* ws, qcp_index* ix) {
+  cudaFree(ws->qwhist);
   cudaFree(ws->boxes);
   cudaFree(ws->items[0]);
   cudaFree(ws->items[1]);

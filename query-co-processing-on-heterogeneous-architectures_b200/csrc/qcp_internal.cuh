@@ -106,6 +106,11 @@ struct Workspace {
   cudaEvent_t ev[kEvCountSlots] = {};
   bool timing = false;
   bool sort_part_marked = false;
+  // per-(query, window) id counts of the sorted path, gathered by the write
+  // pass (hist_G == 0: not gathered, the sort counts them itself)
+  uint32_t* qwhist = nullptr;
+  size_t qwhist_cap = 0;
+  uint32_t hist_G = 0, hist_bits = 0;
   uint32_t blocks_per_sm = 8;    // traversal grid = SMs x this, this call
   uint32_t win_bits = 18;        // sort window, this call
   // CPU + GPU co-processing (QCP_ALGO_HYBRID) of this call
@@ -294,6 +299,11 @@ qcp_status run_batched_device(qcp_index* ix, Workspace* ws, uint32_t q, uint64_t
                               void* sort_tables, cudaStream_t s);
 qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void* tables, cudaStream_t s);
 size_t sort_tables_bytes(const qcp_index* ix, const Workspace* ws, uint32_t q);
+// Window bits and window count of the per-query sort for this call.
+void sort_window_shape(const qcp_index* ix, const Workspace* ws, uint32_t* wbits, uint32_t* G);
+// Largest window count whose per-window counts the write pass gathers.
+constexpr uint32_t kHistMaxG = 256;
+qcp_status ws_reserve_qwhist(Workspace* ws, size_t n);
 // Workspace construction and buffer reservation (qcp_capi.cu).
 qcp_status ws_reserve_queries(qcp_index* ix, Workspace* ws, uint32_t q);
 qcp_status ws_reserve_items(qcp_index* ix, Workspace* ws, size_t items);

@@ -90,6 +90,15 @@ extern "C" qcp_status qcp_plan_create(qcp_index* ix, uint32_t max_queries, uint6
     if ((st = ws_reserve_sort(ix, ws, (size_t)max_queries + 256, (size_t)(max_hits / 4096) + max_queries + 1)) !=
         QCP_OK)
       break;
+    if (p->sort) {  // the write pass gathers the sort's per-window counts
+      uint32_t wbits = 0, G = 0;
+      sort_window_shape(ix, ws, &wbits, &G);
+      if (G <= kHistMaxG) {
+        if ((st = ws_reserve_qwhist(ws, (size_t)max_queries * G)) != QCP_OK) break;
+        ws->hist_G = G;
+        ws->hist_bits = wbits;
+      }
+    }
     if (cudaMalloc(&p->tables, sort_tables_bytes(ix, ws, max_queries)) != cudaSuccess ||
         cudaMalloc(&p->empty, sizeof(float) * row * max_queries) != cudaSuccess) {
       st = cuda_status(cudaGetLastError(), "qcp_plan_create");

@@ -95,8 +95,18 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
                                                   const unsigned long long* __restrict__ offsets,
                                                   unsigned long long* qcursor,
                                                   int32_t* __restrict__ out, uint64_t item_cap,
-                                                  unsigned long long* stats) {
+                                                  unsigned long long* stats, uint32_t* qwhist, uint32_t hist_G,
+                                                  uint32_t hist_bits) {
+  // write pass of the sorted path: per-(query, window) id counts in per-warp
+  // shared counters, flushed once per item
+  __shared__ uint32_t wcount[8][MODE == kWrite ? kHistMaxG : 1];
   const uint32_t lane = threadIdx.x & 31;
+  uint32_t* wc = wcount[(threadIdx.x >> 5) & 7];
+  const bool hist = MODE == kWrite && qwhist != nullptr;
+  if (hist) {
+    for (uint32_t w = lane; w < hist_G; w += 32) wc[w] = 0;
+    __syncwarp();
+  }
   const uint32_t nitems = (uint32_t)min((uint64_t)*item_count, item_cap);
   const uint32_t F = t.fanout;
   const float* lmbr = t.mbr[0];
@@ -160,8 +170,18 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
             out[wpos + j + 32] = b;
             out[wpos + j + 64] = c;
             out[wpos + j + 96] = d;
+            if (hist) {
+              atomicAdd(wc + ((uint32_t)a >> hist_bits), 1u);
+              atomicAdd(wc + ((uint32_t)b >> hist_bits), 1u);
+              atomicAdd(wc + ((uint32_t)c >> hist_bits), 1u);
+              atomicAdd(wc + ((uint32_t)d >> hist_bits), 1u);
+            }
           }
-          for (; j < cnt; j += 32) out[wpos + j] = __ldg(src + j);
+          for (; j < cnt; j += 32) {
+            const int32_t a = __ldg(src + j);
+            out[wpos + j] = a;
+            if (hist) atomicAdd(wc + ((uint32_t)a >> hist_bits), 1u);
+          }
           wpos += cnt;
         }
       }
@@ -187,11 +207,28 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
               if (hm & 2u) out[o++] = idv.y;
               if (hm & 4u) out[o++] = idv.z;
               if (hm & 8u) out[o++] = idv.w;
+              if (hist) {
+                if (hm & 1u) atomicAdd(wc + ((uint32_t)idv.x >> hist_bits), 1u);
+                if (hm & 2u) atomicAdd(wc + ((uint32_t)idv.y >> hist_bits), 1u);
+                if (hm & 4u) atomicAdd(wc + ((uint32_t)idv.z >> hist_bits), 1u);
+                if (hm & 8u) atomicAdd(wc + ((uint32_t)idv.w >> hist_bits), 1u);
+              }
             }
             wpos += tot;
           }
         }
       }
+    }
+    if (hist) {
+      __syncwarp();
+      for (uint32_t w = lane; w < hist_G; w += 32) {
+        const uint32_t c = wc[w];
+        if (c) {
+          atomicAdd(qwhist + (size_t)it.x * hist_G + w, c);
+          wc[w] = 0;
+        }
+      }
+      __syncwarp();
     }
     if (MODE == kCount) {
 #pragma unroll
@@ -359,15 +396,18 @@ void launch_leafscan(bool rect, uint32_t grid, cudaStream_t s, const TreeView& t
                      const uint2* items, const uint32_t* item_count, uint32_t* work,
                      uint32_t* item_hits, uint64_t* qcount, const uint64_t* offsets,
                      uint64_t* qcursor, int32_t* out, uint64_t item_cap,
-                     unsigned long long* stats) {
+                     unsigned long long* stats, uint32_t* qwhist = nullptr, uint32_t hist_G = 0,
+                     uint32_t hist_bits = 0) {
   if (rect)
     k_leafscan<D, true, MODE><<<grid, 256, 0, s>>>(
         t, boxes, items, item_count, work, item_hits, (unsigned long long*)qcount,
-        (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap, stats);
+        (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap, stats, qwhist, hist_G,
+        hist_bits);
   else
     k_leafscan<D, false, MODE><<<grid, 256, 0, s>>>(
         t, boxes, items, item_count, work, item_hits, (unsigned long long*)qcount,
-        (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap, stats);
+        (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap, stats, qwhist, hist_G,
+        hist_bits);
 }
 
 template <int D, int MODE>
@@ -416,7 +456,9 @@ qcp_status write_items(qcp_index* ix, Workspace* ws, int cur, cudaStream_t s) {
   QCP_DISPATCH_D(ix->dims, launch_leafscan<DD, kWrite>(ix->is_rect != 0, grid, s, t, ws->boxes, ws->items[cur],
                                                        ctr + kCtrFrontier0 + cur, ctr + kCtrWork,
                                                        ws->item_hits, nullptr, ws->offsets, ws->qcursor,
-                                                       ws->out_ids, ws->items_cap, ws->d_stats));
+                                                       ws->out_ids, ws->items_cap, ws->d_stats,
+                                                       ws->hist_G ? ws->qwhist : nullptr, ws->hist_G,
+                                                       ws->hist_bits));
   note_launch();
   return check_launch("k_leafscan<write>");
 }
@@ -486,6 +528,17 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
     if (total) {
       QCP_CUDA(cudaMemsetAsync(ws->qcursor, 0, sizeof(uint64_t) * q, s));
       QCP_CUDA(cudaMemsetAsync(ctr + kCtrWork, 0, sizeof(uint32_t), s));
+      ws->hist_G = 0;
+      if (sort) {  // the write pass counts ids per (query, sort window)
+        uint32_t wbits = 0, G = 0;
+        sort_window_shape(ix, ws, &wbits, &G);
+        if (G <= kHistMaxG) {
+          QCP_TRY(ws_reserve_qwhist(ws, (size_t)q * G));
+          QCP_CUDA(cudaMemsetAsync(ws->qwhist, 0, sizeof(uint32_t) * q * G, s));
+          ws->hist_G = G;
+          ws->hist_bits = wbits;
+        }
+      }
       QCP_TRY(write_items(ix, ws, cur, s));
       mark(ws, kEvWrite, s);
       if (sort) QCP_TRY(segmented_sort(ix, ws, q, s));
@@ -520,6 +573,7 @@ qcp_status run_plain(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_only,
   const uint64_t total = *ws->h_total;
   QCP_TRY(ws_reserve_out(ix, ws, (size_t)total));
   if (total) {
+    ws->hist_G = 0;  // the sort counts its windows itself
     QCP_DISPATCH_D(D, launch_mprs<DD, kWrite>(rect, grid, threads, s, t, ws->boxes, q, nullptr,
                                               ws->offsets, ws->out_ids));
     note_launch();
@@ -611,6 +665,7 @@ qcp_status run_batched_device(qcp_index* ix, Workspace* ws, uint32_t q, uint64_t
   note_launch(2);
   QCP_CUDA(cudaMemsetAsync(ws->qcursor, 0, sizeof(uint64_t) * q, s));
   QCP_CUDA(cudaMemsetAsync(ctr + kCtrWork, 0, sizeof(uint32_t), s));
+  if (ws->hist_G) QCP_CUDA(cudaMemsetAsync(ws->qwhist, 0, sizeof(uint32_t) * q * ws->hist_G, s));
   QCP_TRY(write_items(ix, ws, cur, s));
   if (sort) QCP_TRY(segmented_sort_device(ix, ws, q, sort_tables, s));
   return check_launch("batched pipeline (device counts)");

@@ -226,9 +226,12 @@ __global__ void __launch_bounds__(kTileThreads) k_win_hist(const Job* __restrict
 }
 
 // Per job: exclusive scan over its G window counts -> bases and cursors.
+// With qwhist (the write pass's per-(query, window) counts) the job's counts
+// are read from its query's row and copied to whist for k_win_sort.
 __global__ void __launch_bounds__(kTileThreads) k_win_scan(const Job* __restrict__ jobs,
                                                            const uint32_t* __restrict__ njobs_p,
-                                                           uint32_t G, const uint32_t* __restrict__ whist,
+                                                           uint32_t G, uint32_t* __restrict__ whist,
+                                                           const uint32_t* __restrict__ qwhist,
                                                            unsigned long long* wbase,
                                                            unsigned long long* wcur) {
   const uint32_t njobs = *njobs_p;
@@ -238,6 +241,11 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scan(const Job* __restrict
   for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
     const size_t base = (size_t)j * G;
     const uint32_t w0 = threadIdx.x * per;
+    if (qwhist) {
+      const size_t qbase = (size_t)jobs[j].q * G;
+      for (uint32_t k = 0; k < per; ++k)
+        if (w0 + k < G) whist[base + w0 + k] = qwhist[qbase + w0 + k];
+    }
     uint32_t s = 0;
     for (uint32_t k = 0; k < per; ++k)
       if (w0 + k < G) s += whist[base + w0 + k];
@@ -598,13 +606,18 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
     if (st != QCP_OK) break;
     uint32_t* map = ws->seg_hist;
     k_tile_map<<<min(nbig, sms * 8), 256, 0, s>>>(tiles, tile_off, ctr + kCtrJobs1, map);
-    if (cudaMemsetAsync(whist, 0, sizeof(uint32_t) * nw, s) != cudaSuccess) {
-      st = cuda_status(cudaGetLastError(), "memset");
-      break;
+    // per-(job, window) counts: from the write pass when it gathered them
+    const bool have_counts = ws->hist_G == G && ws->hist_bits == wbits;
+    if (!have_counts) {
+      if (cudaMemsetAsync(whist, 0, sizeof(uint32_t) * nw, s) != cudaSuccess) {
+        st = cuda_status(cudaGetLastError(), "memset");
+        break;
+      }
+      k_win_hist<<<min(ntiles, sms * 8), kTileThreads, sizeof(uint32_t) * G, s>>>(
+          big, map, tile_off, ctr + kCtrWork2, ws->out_ids, G, wbits, whist);
     }
-    k_win_hist<<<min(ntiles, sms * 8), kTileThreads, sizeof(uint32_t) * G, s>>>(
-        big, map, tile_off, ctr + kCtrWork2, ws->out_ids, G, wbits, whist);
-    k_win_scan<<<min(nbig, sms * 16), kTileThreads, 0, s>>>(big, ctr + kCtrJobs1, G, whist, wbase, wcur);
+    k_win_scan<<<min(nbig, sms * 16), kTileThreads, 0, s>>>(big, ctr + kCtrJobs1, G, whist,
+                                                            have_counts ? ws->qwhist : nullptr, wbase, wcur);
     k_win_scatter<<<min(ntiles, sms * scatter_blocks_per_sm(scatter_bytes)), kTileThreads, scatter_bytes, s>>>(
         big, map, tile_off, ctr + kCtrWork2, ws->out_ids, ws->tmp_ids, G, wbits, wcur);
     mark(ws, kEvSortPart, s);
@@ -624,6 +637,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
 
 // Window bits and window count of a call (ws->win_bits, bounded as in
 // segmented_sort).
+void sort_window_shape(const qcp_index* ix, const Workspace* ws, uint32_t* wbits, uint32_t* G);
 static void window_shape(const qcp_index* ix, const Workspace* ws, uint32_t* wbits, uint32_t* G) {
   const uint32_t idbits = id_bits(ix->n);
   uint32_t wb = ws->win_bits ? ws->win_bits : kWinBits;
@@ -631,6 +645,10 @@ static void window_shape(const qcp_index* ix, const Workspace* ws, uint32_t* wbi
   if (idbits > 13 && wb < idbits - 13) wb = idbits - 13;
   *wbits = idbits < wb ? idbits : wb;
   *G = 1u << (idbits - *wbits);
+}
+
+void sort_window_shape(const qcp_index* ix, const Workspace* ws, uint32_t* wbits, uint32_t* G) {
+  window_shape(ix, ws, wbits, G);
 }
 
 // Bytes of the per-(job, window) tables that segmented_sort_device needs for
@@ -674,10 +692,14 @@ qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void*
   note_launch(3);
   QCP_TRY(exclusive_scan<uint32_t>(tiles, tile_off, q, ctr + kCtrWork2, ix->pool, s));
   k_tile_map<<<sms * 8, 256, 0, s>>>(tiles, tile_off, ctr + kCtrJobs1, ws->seg_hist);
-  QCP_CUDA(cudaMemsetAsync(whist, 0, sizeof(uint32_t) * nw, s));
-  k_win_hist<<<sms * 8, kTileThreads, sizeof(uint32_t) * G, s>>>(big, ws->seg_hist, tile_off, ctr + kCtrWork2,
-                                                                 ws->out_ids, G, wbits, whist);
-  k_win_scan<<<sms * 16, kTileThreads, 0, s>>>(big, ctr + kCtrJobs1, G, whist, wbase, wcur);
+  const bool have_counts = ws->hist_G == G && ws->hist_bits == wbits;
+  if (!have_counts) {
+    QCP_CUDA(cudaMemsetAsync(whist, 0, sizeof(uint32_t) * nw, s));
+    k_win_hist<<<sms * 8, kTileThreads, sizeof(uint32_t) * G, s>>>(big, ws->seg_hist, tile_off, ctr + kCtrWork2,
+                                                                   ws->out_ids, G, wbits, whist);
+  }
+  k_win_scan<<<sms * 16, kTileThreads, 0, s>>>(big, ctr + kCtrJobs1, G, whist, have_counts ? ws->qwhist : nullptr,
+                                               wbase, wcur);
   k_win_scatter<<<sms * scatter_blocks_per_sm(scatter_bytes), kTileThreads, scatter_bytes, s>>>(
       big, ws->seg_hist, tile_off, ctr + kCtrWork2,
                                                              ws->out_ids, ws->tmp_ids, G, wbits, wcur);
