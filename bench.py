@@ -334,7 +334,9 @@ def run_ours(args, rank, world, local):
                    "batches": int(st["batches"]), "max_inflight": int(st["max_inflight"]),
                    "hits_per_request": round(st["hits"] / max(1, st["requests"]), 1),
                    "output_cap_bytes": 2 << 30, "max_output_bytes": int(st["max_output_bytes"]),
-                   "streams": args.serve_streams}
+                   "streams": args.serve_streams,
+                   "requests_over_10ms": int((lat > 10.0).sum()),
+                   "worst_arrival_s": round(float(t_arr[int(np.argmax(lat))]), 4)}
 
     # ---- captured query plans (CUDA graph replay) vs qcp_query_batch ---------
     plan_out = None
