@@ -26,6 +26,7 @@
 //                              (bits before its word + bits below it in its
 //                              word) -- no comparisons.
 #include "qcp_internal.cuh"
+#include "qcp_tree.cuh"
 
 namespace qcp {
 
@@ -47,10 +48,12 @@ constexpr uint32_t kPerWarpMaxG = 256;  // per-warp window counters up to this G
 constexpr uint32_t kRankThreads = 512;
 constexpr uint32_t kRankWarps = kRankThreads / 32;
 constexpr uint32_t kBmWords = (1u << kWinBits) / 32;  // 8192
-constexpr uint32_t kWarpWords = kBmWords / kRankWarps; // 512 words = 16384 ids: u16 prefixes
-constexpr uint32_t kStage = 6144;                      // staged output ids per window
+constexpr uint32_t kLaneWords = kBmWords / kRankThreads;  // 16 words per thread in the enumeration
+constexpr uint32_t kRankBlocks = 4;                    // resident CTAs per SM
+constexpr uint32_t kStage = 5120;                      // staged output ids per window
 constexpr uint32_t kBatch = 8;                         // ids per thread per load round
 constexpr uint32_t kNone = 0xffffffffu;                // empty register slot
+static_assert(kLaneWords == 16, "k_win_sort reads a thread's words as four 16-byte groups");
 
 using Job = SortJob;
 
@@ -360,36 +363,40 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
 // ============================================================================
 struct RankSmem {
   uint32_t bm[kBmWords];        // one bit per possible id of the window
-  uint16_t pre[kBmWords];       // set bits before each word, within its warp's word range
   int32_t stage[kStage];        // output positions [0, kStage) of the window
-  uint32_t wbase[kRankWarps];   // set bits before each warp's word range
+  uint32_t wsum[kRankWarps];    // set bits in each warp's word range
 };
 
 // Persistent CTAs over the (job, window) pairs g = job * G + window.
 //   1. every id of window g (read from src, the scratch buffer) sets its bit
 //      in a bitmap of the window's 2^wbits possible ids;
-//   2. one sequential pass over the bitmap stores, per 32-bit word, the
-//      number of set bits before it (per warp range, plus warp bases);
-//   3. every id is read again (from L2) and goes to its rank
-//      = bits before its word + popc of its word below its bit;
-//      ranks below kStage are staged in shared memory and leave in
-//      coalesced stores, larger ranks are stored directly.
-// The ids of a window are distinct, so the ranks are a permutation of
-// [0, size) and the window comes out in ascending order.
-__global__ void __launch_bounds__(kRankThreads, 3) k_win_sort(const uint32_t* __restrict__ njobs_p, uint32_t G,
-                                                              uint32_t wbits,
-                                                              const uint32_t* __restrict__ whist,
-                                                              const unsigned long long* __restrict__ wbase,
-                                                              const int32_t* __restrict__ src,
-                                                              int32_t* __restrict__ out) {
+//   2. every thread owns kLaneWords consecutive bitmap words: it counts their
+//      set bits, takes its exclusive prefix over the CTA (warp scan + warp
+//      sums), then walks its nonzero words in order and emits the id of
+//      every set bit at the next rank, clearing each word it read;
+//      ranks below kStage go to a shared-memory stage, larger ones straight
+//      to the output;
+//   3. the stage leaves in coalesced stores.
+// The ids of a window are distinct, so the set bits are the window's ids
+// and their enumeration in bit order is the window in ascending order.
+__global__ void __launch_bounds__(kRankThreads, kRankBlocks) k_win_sort(const uint32_t* __restrict__ njobs_p,
+                                                                        uint32_t G, uint32_t wbits,
+                                                                        const uint32_t* __restrict__ whist,
+                                                                        const unsigned long long* __restrict__ wbase,
+                                                                        const int32_t* __restrict__ src,
+                                                                        int32_t* __restrict__ out) {
   const uint32_t total = *njobs_p * G;  // (job, window) pairs
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RankSmem& s = *reinterpret_cast<RankSmem*>(smem_raw);
   const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   uint4* bm4 = reinterpret_cast<uint4*>(s.bm);
-  const uint32_t nwords = (1u << wbits) >> 5;   // wbits >= 5: slices here hold > 8192 ids
-  const uint32_t ngroups = nwords >> 2;         // groups of 4 words
-  const uint32_t w0 = wp * kWarpWords;          // this warp's word range [w0, w0 + kWarpWords)
+  const uint32_t nwords = (1u << wbits) >> 5;   // wbits >= 12
+  const uint32_t tw0 = tid * kLaneWords;        // this thread's words [tw0, tw0 + kLaneWords)
+  const bool owner = tw0 < nwords;
+  // the four 16-byte groups of a thread's words are read starting at group
+  // (tid >> 1) & 3, so that the 8 threads of a shared-memory phase hit 32
+  // distinct banks
+  const uint32_t rot = (tid >> 1) & 3;
   for (uint32_t i = tid; i < kBmWords / 4; i += kRankThreads) bm4[i] = make_uint4(0, 0, 0, 0);
   __syncthreads();
   for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
@@ -403,82 +410,62 @@ __global__ void __launch_bounds__(kRankThreads, 3) k_win_sort(const uint32_t* __
       if (tid == 0) dst[0] = in[0];
       continue;
     }
-    // 1. set one bit per id (the ids stay in L2 for step 3).  All loads of a
-    //    round are issued before the first atomic: one memory latency per
-    //    4096 ids instead of one per id of the thread.
+    // 1. set one bit per id.  All loads of a round are issued before the
+    //    first atomic; slots past the window's end are skipped per warp.
     for (uint32_t i0 = 0; i0 < size; i0 += kBatch * kRankThreads) {
       uint32_t a[kBatch];
 #pragma unroll
       for (uint32_t k = 0; k < kBatch; ++k) {
         const uint32_t i = i0 + k * kRankThreads + tid;
-        a[k] = i < size ? (uint32_t)in[i] - lo : kNone;
+        a[k] = kNone;
+        if (i0 + k * kRankThreads + (wp << 5) < size && i < size) a[k] = (uint32_t)__ldcs(in + i) - lo;
       }
 #pragma unroll
       for (uint32_t k = 0; k < kBatch; ++k)
-        if (a[k] != kNone) atomicOr(&s.bm[a[k] >> 5], 1u << (a[k] & 31));
+        if (i0 + k * kRankThreads + (wp << 5) < size && a[k] != kNone) atomicOr(&s.bm[a[k] >> 5], 1u << (a[k] & 31));
     }
     __syncthreads();
-    // 2. bits before every word, per warp range
-    uint32_t run = 0;
-    if (w0 < nwords) {
-      for (uint32_t gb = (w0 >> 2); gb < (w0 >> 2) + kWarpWords / 4; gb += 32) {
-        const uint32_t gi = gb + lane;
-        const uint4 q = (gi < ngroups) ? bm4[gi] : make_uint4(0, 0, 0, 0);
-        const uint32_t c0 = __popc(q.x), c1 = __popc(q.y), c2 = __popc(q.z), c3 = __popc(q.w);
-        const uint32_t t = c0 + c1 + c2 + c3;
-        uint32_t x = t;
+    // 2a. set bits and nonzero words of this thread's range
+    uint32_t cnt = 0, nz = 0;
+    if (owner) {
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-          if (lane >= (uint32_t)o) x += y;
-        }
-        const uint32_t e = run + x - t;
-        if (gi < ngroups) {
-          uint2 pk;
-          pk.x = (e & 0xffffu) | ((e + c0) << 16);
-          pk.y = ((e + c0 + c1) & 0xffffu) | ((e + c0 + c1 + c2) << 16);
-          *reinterpret_cast<uint2*>(&s.pre[gi * 4]) = pk;
-        }
-        run += __shfl_sync(0xffffffffu, x, 31);
+      for (uint32_t k = 0; k < 4; ++k) {
+        const uint32_t gi = (k + rot) & 3;
+        const uint4 v = bm4[(tw0 >> 2) + gi];
+        cnt += __popc(v.x) + __popc(v.y) + __popc(v.z) + __popc(v.w);
+        const uint32_t m = (v.x ? 1u : 0u) | (v.y ? 2u : 0u) | (v.z ? 4u : 0u) | (v.w ? 8u : 0u);
+        nz |= m << (gi * 4);
       }
     }
-    if (lane == 0) s.wbase[wp] = run;
+    uint32_t wtot;
+    const uint32_t ex = warp_excl_sum(cnt, &wtot);
+    if (lane == 0) s.wsum[wp] = wtot;
     __syncthreads();
-    if (wp == 0) {
-      const uint32_t v = lane < kRankWarps ? s.wbase[lane] : 0u;
-      uint32_t x = v;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= (uint32_t)o) x += y;
+    // 2b. enumerate the set bits in order
+    const uint32_t ws = lane < kRankWarps ? s.wsum[lane] : 0u;
+    uint32_t pos = __reduce_add_sync(0xffffffffu, lane < wp ? ws : 0u) + ex;
+    // one iteration per set bit (a flat loop: a warp runs as many iterations
+    // as its lane with the most bits); the next nonzero word is fetched, and
+    // cleared, when the current one is used up
+    uint32_t cur = 0, base = 0;
+    for (uint32_t left = cnt; left != 0; --left) {
+      if (cur == 0) {
+        const uint32_t wi = __ffs(nz) - 1;
+        nz &= nz - 1;
+        cur = s.bm[tw0 + wi];
+        s.bm[tw0 + wi] = 0u;
+        base = lo + ((tw0 + wi) << 5);
       }
-      __syncwarp();
-      if (lane < kRankWarps) s.wbase[lane] = x - v;
+      const int32_t id = (int32_t)(base + __ffs(cur) - 1);
+      cur &= cur - 1;
+      if (pos < kStage) s.stage[pos] = id;
+      else dst[pos] = id;
+      ++pos;
     }
     __syncthreads();
-    // 3. every id to its rank
-    for (uint32_t i0 = 0; i0 < size; i0 += kBatch * kRankThreads) {
-      uint32_t a[kBatch];
-#pragma unroll
-      for (uint32_t k = 0; k < kBatch; ++k) {
-        const uint32_t i = i0 + k * kRankThreads + tid;
-        a[k] = i < size ? (uint32_t)__ldcs(in + i) - lo : kNone;
-      }
-#pragma unroll
-      for (uint32_t k = 0; k < kBatch; ++k) {
-        if (a[k] == kNone) continue;
-        const uint32_t wd = a[k] >> 5;
-        const uint32_t r = s.wbase[wd / kWarpWords] + s.pre[wd] + __popc(s.bm[wd] & ((1u << (a[k] & 31)) - 1u));
-        if (r < kStage) s.stage[r] = (int32_t)(a[k] + lo);
-        else dst[r] = (int32_t)(a[k] + lo);
-      }
-    }
-    __syncthreads();
-    // 4. staged ranks out, bitmap cleared
+    // 3. staged ranks out
     const uint32_t ns = size < kStage ? size : kStage;
     for (uint32_t k = tid; k < ns; k += kRankThreads) dst[k] = s.stage[k];
-    for (uint32_t k = tid; k < ngroups; k += kRankThreads) bm4[k] = make_uint4(0, 0, 0, 0);
-    __syncthreads();
   }
 }
 
@@ -622,7 +609,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
         big, map, tile_off, ctr + kCtrWork2, ws->out_ids, ws->tmp_ids, G, wbits, wcur);
     mark(ws, kEvSortPart, s);
     ws->sort_part_marked = ws->timing;
-    const uint32_t grid = (uint32_t)(nw < (uint64_t)sms * 3 ? nw : (uint64_t)sms * 3);
+    const uint32_t grid = (uint32_t)(nw < (uint64_t)sms * kRankBlocks ? nw : (uint64_t)sms * kRankBlocks);
     k_win_sort<<<grid, kRankThreads, rank_bytes, s>>>(ctr + kCtrJobs1, G, wbits, whist, wbase, ws->tmp_ids,
                                                       ws->out_ids);
     note_launch(5);
@@ -703,7 +690,7 @@ qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void*
   k_win_scatter<<<sms * scatter_blocks_per_sm(scatter_bytes), kTileThreads, scatter_bytes, s>>>(
       big, ws->seg_hist, tile_off, ctr + kCtrWork2,
                                                              ws->out_ids, ws->tmp_ids, G, wbits, wcur);
-  k_win_sort<<<sms * 3, kRankThreads, sizeof(RankSmem), s>>>(ctr + kCtrJobs1, G, wbits, whist, wbase,
+  k_win_sort<<<sms * kRankBlocks, kRankThreads, sizeof(RankSmem), s>>>(ctr + kCtrJobs1, G, wbits, whist, wbase,
                                                              ws->tmp_ids, ws->out_ids);
   note_launch(5);
   return check_launch("segmented sort (device counts)");

@@ -21,9 +21,12 @@
 //             output cap next to what other workers hold.
 //
 // Admission by output memory: every worker's plans hold result buffers for
-// at most output_cap / streams bytes of results (ids and offsets), so the
-// results held at once never exceed the cap; requests beyond that run alone
-// under the cap as above.
+// at most output_cap / streams bytes of results (ids and offsets).  Every
+// batch's result bytes are admitted before they are copied out: they wait
+// until they fit under the cap next to what other workers hold, so the
+// results held at once never exceed the cap, except for a request larger
+// than the cap, which is admitted when nothing else is held and so runs
+// alone.
 //
 // Batches on different workers overlap on the device: every worker has its
 // own plans, workspace and stream.  Latency of a request = time its results
@@ -61,6 +64,7 @@ struct ServeState {
   std::mutex mem_mu;
   std::condition_variable mem_cv;
   uint64_t held = 0;        // result bytes admitted and not yet released
+  uint32_t alone_waiting = 0;  // requests above the cap waiting to run alone
 
   // statistics (under mu)
   uint64_t done = 0, hits = 0, batches = 0, batch_sum = 0;
@@ -155,15 +159,35 @@ struct Worker {
     }
   }
 
-  void hold(uint64_t bytes, int delta) {
-    std::lock_guard<std::mutex> g(st.mem_mu);
-    if (delta > 0) {
-      st.held += bytes;
-      std::lock_guard<std::mutex> g2(st.mu);
-      st.max_held = std::max(st.max_held, st.held);
+  // Admission of `bytes` of results: waits until they fit under the cap
+  // next to the results other workers hold, or until nothing is held (a
+  // request larger than the cap then runs alone).  False on a failure.
+  bool admit(uint64_t bytes) {
+    std::unique_lock<std::mutex> lk(st.mem_mu);
+    if (bytes > st.o.output_cap_bytes) {
+      // alone: later batches wait behind it, so that the results held drain
+      ++st.alone_waiting;
+      st.mem_cv.wait(lk, [&] { return st.failed.load() || st.held == 0; });
+      --st.alone_waiting;
     } else {
+      st.mem_cv.wait(lk, [&] {
+        return st.failed.load() ||
+               (st.alone_waiting == 0 && (st.held == 0 || st.held + bytes <= st.o.output_cap_bytes));
+      });
+    }
+    if (st.failed.load()) return false;
+    st.held += bytes;
+    std::lock_guard<std::mutex> g(st.mu);
+    st.max_held = std::max(st.max_held, st.held);
+    return true;
+  }
+
+  void release(uint64_t bytes) {
+    {
+      std::lock_guard<std::mutex> g(st.mem_mu);
       st.held -= bytes;
     }
+    st.mem_cv.notify_all();
   }
 
   // requests batch[first, first + nb) through a plan; false on a failure
@@ -190,20 +214,19 @@ struct Worker {
       return false;
     }
     const uint64_t bytes = total * 4 + ((uint64_t)nb + 1) * 8;
-    hold(bytes, +1);
+    if (!admit(bytes)) return false;
     if (cudaMemcpyAsync(r.h_offs, d_offs, sizeof(uint64_t) * ((size_t)nb + 1), cudaMemcpyDeviceToHost, r.stream) !=
             cudaSuccess ||
         (total && cudaMemcpyAsync(r.h_ids, d_ids, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, r.stream) !=
                       cudaSuccess) ||
         cudaStreamSynchronize(r.stream) != cudaSuccess) {
-      hold(bytes, -1);
+      release(bytes);
       fail(st, qcp::cuda_status(cudaGetLastError(), "serve result copy"));
       return false;
     }
     const Clock::time_point now = Clock::now();
     finish(first, nb, r.h_offs, r.h_ids, now);
-    hold(bytes, -1);
-    st.mem_cv.notify_all();
+    release(bytes);
     account(nb, total, now);
     return true;
   }
@@ -223,22 +246,13 @@ struct Worker {
     }
     uint64_t bytes = ((uint64_t)nb + 1) * 8;
     for (uint32_t k = 0; k < nb; ++k) bytes += counts[k] * 4;
-    {
-      std::unique_lock<std::mutex> lk(st.mem_mu);
-      st.mem_cv.wait(lk, [&] {
-        return st.failed.load() || st.held == 0 || st.held + bytes <= st.o.output_cap_bytes;
-      });
-      if (st.failed.load()) return false;
-      st.held += bytes;
-      std::lock_guard<std::mutex> g(st.mu);
-      st.max_held = std::max(st.max_held, st.held);
-    }
+    if (!admit(bytes)) return false;
     qcp_result res;
     memset(&res, 0, sizeof(res));
     s = qcp_query_batch(st.ix, b, nb, &qo, &res);
     const Clock::time_point now = Clock::now();
     if (s != QCP_OK) {
-      hold(bytes, -1);
+      release(bytes);
       fail(st, s);
       return false;
     }
@@ -246,8 +260,7 @@ struct Worker {
            now);
     const uint64_t total = res.total_hits;
     qcp_result_release(&res);
-    hold(bytes, -1);
-    st.mem_cv.notify_all();
+    release(bytes);
     account(nb, total, now);
     return true;
   }
