@@ -49,8 +49,9 @@ constexpr uint32_t kRankThreads = 512;
 constexpr uint32_t kRankWarps = kRankThreads / 32;
 constexpr uint32_t kBmWords = (1u << kWinBits) / 32;  // 8192
 constexpr uint32_t kLaneWords = kBmWords / kRankThreads;  // 16 words per thread in the enumeration
-constexpr uint32_t kRankBlocks = 4;                    // resident CTAs per SM
-constexpr uint32_t kStage = 5120;                      // staged output ids per window
+constexpr uint32_t kRankBlocks = 3;                    // resident CTAs per SM
+constexpr uint32_t kStage = 6144;                      // staged output ids per window
+constexpr uint32_t kPrefetch = 4096;                   // ids of the next window loaded ahead
 constexpr uint32_t kBatch = 8;                         // ids per thread per load round
 constexpr uint32_t kNone = 0xffffffffu;                // empty register slot
 static_assert(kLaneWords == 16, "k_win_sort reads a thread's words as four 16-byte groups");
@@ -364,12 +365,23 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
 struct RankSmem {
   uint32_t bm[kBmWords];        // one bit per possible id of the window
   int32_t stage[kStage];        // output positions [0, kStage) of the window
+  int32_t pf[kPrefetch];        // first ids of the next window, loaded ahead
   uint32_t wsum[kRankWarps];    // set bits in each warp's word range
 };
 
+// 4-byte global -> shared copies that run behind the CTA's other work
+// (cp.async, waited for with cp_async_wait_all before the data is read).
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // Persistent CTAs over the (job, window) pairs g = job * G + window.
 //   1. every id of window g (read from src, the scratch buffer) sets its bit
-//      in a bitmap of the window's 2^wbits possible ids;
+//      in a bitmap of the window's 2^wbits possible ids; its first kPrefetch
+//      ids were copied to shared memory while the previous window ran;
 //   2. every thread owns kLaneWords consecutive bitmap words: it counts their
 //      set bits, takes its exclusive prefix over the CTA (warp scan + warp
 //      sums), then walks its nonzero words in order and emits the id of
@@ -399,32 +411,65 @@ __global__ void __launch_bounds__(kRankThreads, kRankBlocks) k_win_sort(const ui
   const uint32_t rot = (tid >> 1) & 3;
   for (uint32_t i = tid; i < kBmWords / 4; i += kRankThreads) bm4[i] = make_uint4(0, 0, 0, 0);
   __syncthreads();
+  // the first kPrefetch ids of window g + gridDim.x are copied into s.pf
+  // while window g is enumerated
+  uint32_t size = 0;
+  unsigned long long off = 0;
+  if (blockIdx.x < total) {
+    size = whist[blockIdx.x];
+    off = wbase[blockIdx.x];
+    const uint32_t n = size < kPrefetch ? size : kPrefetch;
+    for (uint32_t i = tid; i < n; i += kRankThreads) cp_async4(&s.pf[i], src + off + i);
+  }
+  cp_async_commit();
   for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
-    const uint32_t size = whist[g];
-    if (size == 0) continue;
-    const unsigned long long off = wbase[g];
+    const uint32_t gn = g + gridDim.x;
+    uint32_t nsize = 0;
+    unsigned long long noff = 0;
+    if (gn < total) {
+      nsize = whist[gn];
+      noff = wbase[gn];
+    }
     const int32_t* in = src + off;
     int32_t* dst = out + off;
     const uint32_t lo = (g % G) << wbits;
-    if (size == 1) {
-      if (tid == 0) dst[0] = in[0];
-      continue;
-    }
-    // 1. set one bit per id.  All loads of a round are issued before the
-    //    first atomic; slots past the window's end are skipped per warp.
-    for (uint32_t i0 = 0; i0 < size; i0 += kBatch * kRankThreads) {
-      uint32_t a[kBatch];
-#pragma unroll
-      for (uint32_t k = 0; k < kBatch; ++k) {
-        const uint32_t i = i0 + k * kRankThreads + tid;
-        a[k] = kNone;
-        if (i0 + k * kRankThreads + (wp << 5) < size && i < size) a[k] = (uint32_t)__ldcs(in + i) - lo;
+    cp_async_wait_all();
+    __syncthreads();  // this window's prefetched ids are visible to every thread
+    // 1. set one bit per id: the prefetched ones from shared memory, the
+    //    rest in rounds whose loads are all issued before the first atomic
+    if (size >= 2) {
+      const uint32_t npf = size < kPrefetch ? size : kPrefetch;
+      for (uint32_t i = tid; i < npf; i += kRankThreads) {
+        const uint32_t x = (uint32_t)s.pf[i] - lo;
+        atomicOr(&s.bm[x >> 5], 1u << (x & 31));
       }
+      for (uint32_t i0 = kPrefetch; i0 < size; i0 += kBatch * kRankThreads) {
+        uint32_t a[kBatch];
 #pragma unroll
-      for (uint32_t k = 0; k < kBatch; ++k)
-        if (i0 + k * kRankThreads + (wp << 5) < size && a[k] != kNone) atomicOr(&s.bm[a[k] >> 5], 1u << (a[k] & 31));
+        for (uint32_t k = 0; k < kBatch; ++k) {
+          const uint32_t i = i0 + k * kRankThreads + tid;
+          a[k] = kNone;
+          if (i0 + k * kRankThreads + (wp << 5) < size && i < size) a[k] = (uint32_t)__ldcs(in + i) - lo;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kBatch; ++k)
+          if (i0 + k * kRankThreads + (wp << 5) < size && a[k] != kNone)
+            atomicOr(&s.bm[a[k] >> 5], 1u << (a[k] & 31));
+      }
+    } else if (size == 1 && tid == 0) {
+      dst[0] = s.pf[0];
     }
-    __syncthreads();
+    __syncthreads();  // bitmap complete; s.pf free
+    {
+      const uint32_t n = nsize < kPrefetch ? nsize : kPrefetch;
+      for (uint32_t i = tid; i < n; i += kRankThreads) cp_async4(&s.pf[i], src + noff + i);
+      cp_async_commit();
+    }
+    if (size < 2) {
+      size = nsize;
+      off = noff;
+      continue;  // uniform over the CTA
+    }
     // 2a. set bits and nonzero words of this thread's range
     uint32_t cnt = 0, nz = 0;
     if (owner) {
@@ -466,7 +511,10 @@ __global__ void __launch_bounds__(kRankThreads, kRankBlocks) k_win_sort(const ui
     // 3. staged ranks out
     const uint32_t ns = size < kStage ? size : kStage;
     for (uint32_t k = tid; k < ns; k += kRankThreads) dst[k] = s.stage[k];
+    size = nsize;
+    off = noff;
   }
+  cp_async_wait_all();
 }
 
 }  // namespace
