@@ -295,10 +295,26 @@ qcp_status qcp_plan_free(qcp_plan* plan);
  * the other workers hold.  Plans and buffers are set up before the clock
  * starts.  deliver (optional) receives every request's ascending ids, from
  * the worker threads, once each.  latency_ms (optional, q entries) gets
- * arrival -> results-on-host time per request.  No counterpart in the
- * reference (its Evaluator replays fixed query files through Tree::Search,
- * src/evaluator/evaluator.cpp:171-280). */
+ * arrival -> results-on-host time per request; trace (optional) gets one
+ * qcp_serve_batch per run, in completion order (stats->batches runs in all).
+ * No counterpart in the reference (its Evaluator replays fixed query files
+ * through Tree::Search, src/evaluator/evaluator.cpp:171-280). */
 typedef void (*qcp_deliver_fn)(void* user, uint32_t request, const int32_t* ids, uint64_t n);
+
+/* One plan replay (or one alone run) of a serving replay, recorded when
+ * qcp_serve_opts.trace is set.  Times are seconds since the replay started. */
+typedef struct qcp_serve_batch {
+  uint32_t worker;     /* worker thread (stream) index */
+  uint32_t requests;   /* requests in this run */
+  uint32_t path;       /* 0: small plan, 1: large plan, 2: alone through qcp_query_batch */
+  uint32_t split;      /* 1: part of a batch split after an overflow */
+  uint64_t hits;
+  double t_taken;      /* the batch was taken from the queue */
+  double t_start;      /* this run started */
+  double t_run;        /* this run's hit total was on the host */
+  double t_admitted;   /* its result bytes were admitted under the cap */
+  double t_done;       /* its results were on the host and delivered */
+} qcp_serve_batch;
 
 typedef struct qcp_serve_opts {
   uint32_t streams;          /* batches in flight; 0 = 4 */
@@ -306,6 +322,8 @@ typedef struct qcp_serve_opts {
   uint64_t output_cap_bytes; /* result bytes held at once; 0 = 2 GiB */
   qcp_deliver_fn deliver;    /* NULL: results are dropped after the copy */
   void* user;                /* passed to deliver */
+  qcp_serve_batch* trace;    /* NULL, or room for trace_cap records (the first ones are kept) */
+  uint64_t trace_cap;
 } qcp_serve_opts;
 
 typedef struct qcp_serve_stats {

@@ -83,7 +83,20 @@ DELIVER_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.POI
 class ServeOpts(ctypes.Structure):
     _fields_ = [("streams", ctypes.c_uint32), ("max_batch", ctypes.c_uint32),
                 ("output_cap_bytes", ctypes.c_uint64), ("deliver", DELIVER_FN),
-                ("user", ctypes.c_void_p)]
+                ("user", ctypes.c_void_p), ("trace", ctypes.c_void_p), ("trace_cap", ctypes.c_uint64)]
+
+
+class ServeBatch(ctypes.Structure):
+    """qcp_serve_batch: one run of a serving replay (times in seconds)."""
+    _fields_ = [("worker", ctypes.c_uint32), ("requests", ctypes.c_uint32), ("path", ctypes.c_uint32),
+                ("split", ctypes.c_uint32), ("hits", ctypes.c_uint64), ("t_taken", ctypes.c_double),
+                ("t_start", ctypes.c_double), ("t_run", ctypes.c_double), ("t_admitted", ctypes.c_double),
+                ("t_done", ctypes.c_double)]
+
+
+# numpy view of an array of qcp_serve_batch records
+SERVE_BATCH_DTYPE = np.dtype([(n, {ctypes.c_uint32: "<u4", ctypes.c_uint64: "<u8", ctypes.c_double: "<f8"}[t])
+                              for n, t in ServeBatch._fields_])
 
 
 class ServeStats(ctypes.Structure):
@@ -358,12 +371,13 @@ class Index:
 
 
     def serve(self, boxes, arrival_s, streams: int = 4, max_batch: int = 16384,
-              output_cap_bytes: int = 2 << 30, collect: bool = False):
+              output_cap_bytes: int = 2 << 30, collect: bool = False, trace: int = 0):
         """Replay an open-loop arrival trace through the library's continuous
         batching loop (qcp_serve_replay).  boxes: (q, 2*dims) float32 host
         array; arrival_s: non-decreasing arrival times in seconds.  Returns
         (stats dict, per-request latency in ms, per-request id arrays or
-        None when collect is False)."""
+        None when collect is False).  With trace > 0, stats["trace"] holds
+        the first `trace` runs as a SERVE_BATCH_DTYPE array."""
         lib = load_library()
         b = np.ascontiguousarray(boxes, dtype=np.float32).reshape(-1, 2 * self.dims)
         t = np.ascontiguousarray(arrival_s, dtype=np.float64)
@@ -373,6 +387,9 @@ class Index:
         got = [None] * b.shape[0] if collect else None
         opts = ServeOpts()
         opts.streams, opts.max_batch, opts.output_cap_bytes = streams, max_batch, output_cap_bytes
+        tr = np.zeros(int(trace), SERVE_BATCH_DTYPE) if trace > 0 else None
+        if tr is not None:
+            opts.trace, opts.trace_cap = tr.ctypes.data, tr.shape[0]
         if collect:
             import threading
             lock = threading.Lock()
@@ -387,6 +404,8 @@ class Index:
         _check(lib.qcp_serve_replay(self._h, _ptr(b), _ptr(t), b.shape[0], ctypes.byref(opts), _ptr(lat),
                                     ctypes.byref(st)))
         stats = {k: getattr(st, k) for k, _ in ServeStats._fields_ if k != "reserved_"}
+        if tr is not None:
+            stats["trace"] = tr[:min(int(st.batches), tr.shape[0])]
         return stats, lat, got
 
 

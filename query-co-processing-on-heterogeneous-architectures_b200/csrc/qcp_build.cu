@@ -426,13 +426,29 @@ void temp_free(void* p, cudaStream_t s) {
   if (p) cudaFreeAsync(p, s);
 }
 
+size_t scan_scratch_bytes(uint64_t n) {
+  return sizeof(uint64_t) * (size_t)((n + SC_CHUNK - 1) / SC_CHUNK + 1);
+}
+
+// The chunk sums live in `scratch` when the caller passes one (at least
+// scan_scratch_bytes(n) bytes), else in a stream-ordered temporary.  Captured
+// pipelines pass scratch: a temporary would become a graph memory node,
+// whose physical memory the driver maps at a launch that needs more of it
+// than the graphs already running hold.
 template <class T>
 qcp_status exclusive_scan(const T* in, T* out, uint64_t n, T* grand_total, DevPool& pool,
-                          cudaStream_t s) {
+                          cudaStream_t s, void* scratch, size_t scratch_bytes) {
   (void)pool;
   const uint32_t nblk = (uint32_t)((n + SC_CHUNK - 1) / SC_CHUNK);
-  void* sums = nullptr;
-  QCP_TRY(temp_alloc(sizeof(T) * (nblk ? nblk : 1), s, &sums));
+  void* sums = scratch;
+  if (scratch) {
+    if (scratch_bytes < sizeof(T) * (nblk ? nblk : 1)) {
+      set_error("exclusive_scan: scratch too small");
+      return QCP_ERR_BAD_ARG;
+    }
+  } else {
+    QCP_TRY(temp_alloc(sizeof(T) * (nblk ? nblk : 1), s, &sums));
+  }
   if (n) {
     k_scan_sums<T><<<nblk, SC_THREADS, 0, s>>>(in, n, (T*)sums);
     k_scan_partials<T><<<1, 1024, 0, s>>>((T*)sums, nblk, grand_total);
@@ -440,14 +456,14 @@ qcp_status exclusive_scan(const T* in, T* out, uint64_t n, T* grand_total, DevPo
     note_launch(3);
   }
   qcp_status st = check_launch("exclusive_scan");
-  temp_free(sums, s);
+  if (!scratch) temp_free(sums, s);
   return st;
 }
 
 template qcp_status exclusive_scan<uint32_t>(const uint32_t*, uint32_t*, uint64_t, uint32_t*,
-                                             DevPool&, cudaStream_t);
+                                             DevPool&, cudaStream_t, void*, size_t);
 template qcp_status exclusive_scan<uint64_t>(const uint64_t*, uint64_t*, uint64_t, uint64_t*,
-                                             DevPool&, cudaStream_t);
+                                             DevPool&, cudaStream_t, void*, size_t);
 
 qcp_status build_keys(const float* objs, uint64_t n, uint32_t dims, uint32_t is_rect,
                       uint32_t key_mode, uint32_t key_bits, uint64_t* keys, uint32_t* vals,
@@ -524,13 +540,13 @@ qcp_status build_levels(qcp_index* ix, cudaStream_t s) {
 }
 
 qcp_status exclusive_scan_counts(const uint64_t* counts, uint64_t* offsets, uint32_t q,
-                                 DevPool& pool, cudaStream_t s) {
+                                 DevPool& pool, cudaStream_t s, void* scratch, size_t scratch_bytes) {
   // offsets has q+1 entries; offsets[q] receives the total.
   if (q == 0) {
     QCP_CUDA(cudaMemsetAsync(offsets, 0, sizeof(uint64_t), s));
     return QCP_OK;
   }
-  return exclusive_scan<uint64_t>(counts, offsets, q, offsets + q, pool, s);
+  return exclusive_scan<uint64_t>(counts, offsets, q, offsets + q, pool, s, scratch, scratch_bytes);
 }
 
 }  // namespace qcp

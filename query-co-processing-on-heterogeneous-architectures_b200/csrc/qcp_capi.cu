@@ -299,6 +299,7 @@ qcp_status ws_reserve_qwhist(Workspace* ws, size_t n) {
 
 void ws_destroy(Workspace* ws, qcp_index* ix) {
   cudaFree(ws->qwhist);
+  cudaFree(ws->scan_tmp);
   cudaFree(ws->boxes);
   cudaFree(ws->items[0]);
   cudaFree(ws->items[1]);

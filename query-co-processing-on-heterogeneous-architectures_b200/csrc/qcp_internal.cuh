@@ -110,6 +110,8 @@ struct Workspace {
   // pass (hist_G == 0: not gathered, the sort counts them itself)
   uint32_t* qwhist = nullptr;
   size_t qwhist_cap = 0;
+  void* scan_tmp = nullptr;  // scan chunk sums of the captured pipeline (plans)
+  size_t scan_tmp_cap = 0;
   uint32_t hist_G = 0, hist_bits = 0;
   uint32_t blocks_per_sm = 8;    // traversal grid = SMs x this, this call
   uint32_t win_bits = 18;        // sort window, this call
@@ -320,9 +322,12 @@ qcp_status run_batched_counts_into(qcp_index* ix, const float* boxes, uint32_t q
                                    uint2* items0, uint2* items1, uint32_t* item_hits, size_t item_cap,
                                    uint32_t* ctr, unsigned long long* stats, cudaStream_t s);
 qcp_status exclusive_scan_counts(const uint64_t* counts, uint64_t* offsets, uint32_t q,
-                                 DevPool& pool, cudaStream_t s);
+                                 DevPool& pool, cudaStream_t s, void* scratch = nullptr,
+                                 size_t scratch_bytes = 0);
 template <class T>
 qcp_status exclusive_scan(const T* in, T* out, uint64_t n, T* grand_total, DevPool& pool,
-                          cudaStream_t s);
+                          cudaStream_t s, void* scratch = nullptr, size_t scratch_bytes = 0);
+// Bytes of caller-owned scratch an exclusive scan of n values needs.
+size_t scan_scratch_bytes(uint64_t n);
 
 }  // namespace qcp

@@ -99,7 +99,10 @@ extern "C" qcp_status qcp_plan_create(qcp_index* ix, uint32_t max_queries, uint6
         ws->hist_bits = wbits;
       }
     }
-    if (cudaMalloc(&p->tables, sort_tables_bytes(ix, ws, max_queries)) != cudaSuccess ||
+    // scan scratch owned by the workspace: no stream-ordered temporaries in the graph
+    ws->scan_tmp_cap = scan_scratch_bytes((uint64_t)max_queries + 1);
+    if (cudaMalloc(&ws->scan_tmp, ws->scan_tmp_cap) != cudaSuccess ||
+        cudaMalloc(&p->tables, sort_tables_bytes(ix, ws, max_queries)) != cudaSuccess ||
         cudaMalloc(&p->empty, sizeof(float) * row * max_queries) != cudaSuccess) {
       st = cuda_status(cudaGetLastError(), "qcp_plan_create");
       break;
@@ -113,8 +116,7 @@ extern "C" qcp_status qcp_plan_create(qcp_index* ix, uint32_t max_queries, uint6
       st = cuda_status(cudaGetLastError(), "qcp_plan_create");
       break;
     }
-    // one plain run first: kernel attributes and the stream-ordered pool are
-    // set up outside the capture
+    // one plain run first: kernel attributes are set up outside the capture
     if ((st = run_batched_device(ix, ws, max_queries, max_hits, p->sort, p->tables, p->capture)) != QCP_OK) break;
     if (cudaStreamSynchronize(p->capture) != cudaSuccess) {
       st = cuda_status(cudaGetLastError(), "qcp_plan_create warm-up");
@@ -130,8 +132,43 @@ extern "C" qcp_status qcp_plan_create(qcp_index* ix, uint32_t max_queries, uint6
       st = cs;
       break;
     }
-    if (ce != cudaSuccess || cudaGraphInstantiate(&p->exec, p->graph, 0) != cudaSuccess) {
+    if (ce != cudaSuccess) {
       st = cuda_status(cudaGetLastError(), "qcp_plan_create graph");
+      break;
+    }
+    // the pipeline must not allocate inside the graph: the physical memory of
+    // a graph memory node is mapped at whichever launch first needs more of
+    // it than the graphs already running hold, which stalled replays of
+    // concurrent plans for hundreds of milliseconds
+    {
+      size_t nn = 0;
+      std::vector<cudaGraphNode_t> nodes;
+      if (cudaGraphGetNodes(p->graph, nullptr, &nn) == cudaSuccess) {
+        nodes.resize(nn);
+        if (nn && cudaGraphGetNodes(p->graph, nodes.data(), &nn) != cudaSuccess) nn = 0;
+      }
+      bool mem_node = false;
+      for (size_t k = 0; k < nn; ++k) {
+        cudaGraphNodeType ty;
+        if (cudaGraphNodeGetType(nodes[k], &ty) == cudaSuccess &&
+            (ty == cudaGraphNodeTypeMemAlloc || ty == cudaGraphNodeTypeMemFree))
+          mem_node = true;
+      }
+      if (mem_node) {
+        set_error("qcp_plan_create: the captured pipeline holds a memory allocation node");
+        st = QCP_ERR_CUDA;
+        break;
+      }
+    }
+    if (cudaGraphInstantiate(&p->exec, p->graph, 0) != cudaSuccess) {
+      st = cuda_status(cudaGetLastError(), "qcp_plan_create graph");
+      break;
+    }
+    // one replay of the empty batch (ws->boxes still holds it): the graph's
+    // first launch uploads it, which would otherwise land on the first real
+    // batch
+    if (cudaGraphLaunch(p->exec, p->capture) != cudaSuccess || cudaStreamSynchronize(p->capture) != cudaSuccess) {
+      st = cuda_status(cudaGetLastError(), "qcp_plan_create first replay");
       break;
     }
   } while (false);

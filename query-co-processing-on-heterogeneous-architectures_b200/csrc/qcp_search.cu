@@ -658,7 +658,7 @@ qcp_status run_batched_device(qcp_index* ix, Workspace* ws, uint32_t q, uint64_t
                                                 ws->qcount, nullptr, nullptr, nullptr, ws->items_cap,
                                                 ws->d_stats));
   note_launch();
-  QCP_TRY(exclusive_scan_counts(ws->qcount, ws->offsets, q, ix->pool, s));
+  QCP_TRY(exclusive_scan_counts(ws->qcount, ws->offsets, q, ix->pool, s, ws->scan_tmp, ws->scan_tmp_cap));
   k_gate<<<1, 32, 0, s>>>((const unsigned long long*)ws->offsets, q, ids_cap, ctr + kCtrFrontier0 + cur,
                           ctr + kCtrOverflow);
   k_gate_zero<<<(q + 256) / 256, 256, 0, s>>>((unsigned long long*)ws->offsets, q, ctr + kCtrOverflow);

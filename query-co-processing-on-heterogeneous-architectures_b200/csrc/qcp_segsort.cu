@@ -725,7 +725,8 @@ qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void*
   k_sort_small<<<sms * 3, kSmallThreads, sizeof(BucketSmem), s>>>(small, ctr + kCtrJobs0, ws->out_ids, idbits);
   k_tiles_per_job<<<(q + 255) / 256, 256, 0, s>>>(big, ctr + kCtrJobs1, q, tiles);
   note_launch(3);
-  QCP_TRY(exclusive_scan<uint32_t>(tiles, tile_off, q, ctr + kCtrWork2, ix->pool, s));
+  QCP_TRY(exclusive_scan<uint32_t>(tiles, tile_off, q, ctr + kCtrWork2, ix->pool, s, ws->scan_tmp,
+                                   ws->scan_tmp_cap));
   k_tile_map<<<sms * 8, 256, 0, s>>>(tiles, tile_off, ctr + kCtrJobs1, ws->seg_hist);
   const bool have_counts = ws->hist_G == G && ws->hist_bits == wbits;
   if (!have_counts) {

@@ -66,6 +66,8 @@ struct ServeState {
   uint64_t held = 0;        // result bytes admitted and not yet released
   uint32_t alone_waiting = 0;  // requests above the cap waiting to run alone
 
+  std::atomic<uint64_t> trace_next{0};  // next qcp_serve_batch record
+
   // statistics (under mu)
   uint64_t done = 0, hits = 0, batches = 0, batch_sum = 0;
   uint32_t inflight = 0, max_inflight = 0;
@@ -140,6 +142,27 @@ struct Worker {
   std::vector<float> boxes;      // gathered boxes of the current batch
   std::vector<uint32_t> batch;   // request indices of the current batch
   std::vector<uint64_t> counts;
+  uint32_t index = 0;     // worker index
+  double t_taken = 0.0;   // the current batch left the queue
+
+  // one qcp_serve_batch record, if tracing
+  void record(uint32_t nb, uint32_t path, uint32_t split, uint64_t total, double t_start, double t_run,
+              double t_admitted, double t_done) {
+    if (!st.o.trace) return;
+    const uint64_t k = st.trace_next.fetch_add(1);
+    if (k >= st.o.trace_cap) return;
+    qcp_serve_batch& b = st.o.trace[k];
+    b.worker = index;
+    b.requests = nb;
+    b.path = path;
+    b.split = split;
+    b.hits = total;
+    b.t_taken = t_taken;
+    b.t_start = t_start;
+    b.t_run = t_run;
+    b.t_admitted = t_admitted;
+    b.t_done = t_done;
+  }
 
   void account(uint32_t nb, uint64_t total, Clock::time_point now) {
     std::lock_guard<std::mutex> g(st.mu);
@@ -191,30 +214,34 @@ struct Worker {
   }
 
   // requests batch[first, first + nb) through a plan; false on a failure
-  bool run_planned(uint32_t first, uint32_t nb) {
+  bool run_planned(uint32_t first, uint32_t nb, uint32_t split) {
     const uint32_t pmax = r.plans[1] ? r.plan_q[1] : r.plan_q[0];
     if (nb > pmax) {  // larger than the largest plan: consecutive chunks
       for (uint32_t c = 0; c < nb; c += pmax)
-        if (!run_planned(first + c, nb - c < pmax ? nb - c : pmax)) return false;
+        if (!run_planned(first + c, nb - c < pmax ? nb - c : pmax, split)) return false;
       return true;
     }
-    qcp_plan* plan = (nb <= r.plan_q[0]) ? r.plans[0] : r.plans[1];
+    const uint32_t path = (nb <= r.plan_q[0]) ? 0u : 1u;
+    qcp_plan* plan = r.plans[path];
     uint64_t total = 0;
     const uint64_t* d_offs = nullptr;
     const int32_t* d_ids = nullptr;
     const float* b = boxes.data() + (size_t)first * st.dims2;
+    const double t_start = since(st, Clock::now());
     qcp_status s = qcp_plan_run(plan, b, nb, QCP_MEM_HOST, r.stream, &total, &d_offs, &d_ids);
     if (s == QCP_ERR_OUTPUT_OVERFLOW) {  // split and replay
-      if (nb == 1) return run_direct(first, 1);
+      if (nb == 1) return run_direct(first, 1, 1);
       const uint32_t h = nb / 2;
-      return run_planned(first, h) && run_planned(first + h, nb - h);
+      return run_planned(first, h, 1) && run_planned(first + h, nb - h, 1);
     }
     if (s != QCP_OK) {
       fail(st, s);
       return false;
     }
+    const double t_run = since(st, Clock::now());
     const uint64_t bytes = total * 4 + ((uint64_t)nb + 1) * 8;
     if (!admit(bytes)) return false;
+    const double t_admitted = since(st, Clock::now());
     if (cudaMemcpyAsync(r.h_offs, d_offs, sizeof(uint64_t) * ((size_t)nb + 1), cudaMemcpyDeviceToHost, r.stream) !=
             cudaSuccess ||
         (total && cudaMemcpyAsync(r.h_ids, d_ids, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, r.stream) !=
@@ -228,25 +255,29 @@ struct Worker {
     finish(first, nb, r.h_offs, r.h_ids, now);
     release(bytes);
     account(nb, total, now);
+    record(nb, path, split, total, t_start, t_run, t_admitted, since(st, now));
     return true;
   }
 
   // requests batch[first, first + nb) through qcp_query_batch, admitted by
   // their counted result bytes against the output cap
-  bool run_direct(uint32_t first, uint32_t nb) {
+  bool run_direct(uint32_t first, uint32_t nb, uint32_t split) {
     qcp_query_opts qo;
     memset(&qo, 0, sizeof(qo));
     qo.stream = r.stream;
     const float* b = boxes.data() + (size_t)first * st.dims2;
     counts.resize(nb);
+    const double t_start = since(st, Clock::now());
     qcp_status s = qcp_query_counts(st.ix, b, nb, &qo, counts.data());
     if (s != QCP_OK) {
       fail(st, s);
       return false;
     }
+    const double t_run = since(st, Clock::now());
     uint64_t bytes = ((uint64_t)nb + 1) * 8;
     for (uint32_t k = 0; k < nb; ++k) bytes += counts[k] * 4;
     if (!admit(bytes)) return false;
+    const double t_admitted = since(st, Clock::now());
     qcp_result res;
     memset(&res, 0, sizeof(res));
     s = qcp_query_batch(st.ix, b, nb, &qo, &res);
@@ -262,6 +293,7 @@ struct Worker {
     qcp_result_release(&res);
     release(bytes);
     account(nb, total, now);
+    record(nb, 2, split, total, t_start, t_run, t_admitted, since(st, now));
     return true;
   }
 
@@ -285,11 +317,12 @@ struct Worker {
         ++st.inflight;
         st.max_inflight = std::max(st.max_inflight, st.inflight);
       }
+      t_taken = since(st, Clock::now());
       const uint32_t nb = (uint32_t)batch.size();
       for (uint32_t k = 0; k < nb; ++k)
         std::copy(st.boxes + (size_t)batch[k] * st.dims2, st.boxes + (size_t)(batch[k] + 1) * st.dims2,
                   boxes.begin() + (size_t)k * st.dims2);
-      const bool ok = r.plans[0] ? run_planned(0, nb) : run_direct(0, nb);
+      const bool ok = r.plans[0] ? run_planned(0, nb, 0) : run_direct(0, nb, 0);
       {
         std::lock_guard<std::mutex> g(st.mu);
         --st.inflight;
@@ -343,7 +376,7 @@ extern "C" qcp_status qcp_serve_replay(qcp_index* ix, const float* boxes, const 
   for (uint32_t w = 0; w < st.o.streams; ++w)
     pool.emplace_back([&st, &res, w, dev] {
       cudaSetDevice(dev);
-      Worker wk{st, res[w], {}, {}, {}};
+      Worker wk{st, res[w], {}, {}, {}, w, 0.0};
       wk.loop();
     });
   // feeder: open-loop arrivals

@@ -52,3 +52,37 @@ def test_python_binding_fails_loudly_without_library(qcp, tmp_path):
 
 def test_version(qcp):
     assert qcp.load_library().qcp_version().startswith(b"qcp-b200")
+
+
+STRUCTS = [("BuildOpts", "qcp_build_opts"), ("IndexInfo", "qcp_index_info"), ("QueryOpts", "qcp_query_opts"),
+           ("QueryStats", "qcp_query_stats"), ("Result", "qcp_result"), ("TuneResult", "qcp_tune_result"),
+           ("ServeOpts", "qcp_serve_opts"), ("ServeStats", "qcp_serve_stats"), ("ServeBatch", "qcp_serve_batch")]
+
+
+def test_binding_struct_layouts_match_header(qcp, tmp_path):
+    """Every ctypes mirror of a qcp.h struct has the C compiler's size and
+    field offsets (a C program built against the header prints them)."""
+    import shutil
+    import subprocess
+    if not shutil.which("gcc"):
+        pytest.skip("gcc not found")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "qcp.h"', "int main(void) {"]
+    for py, c in STRUCTS:
+        lines.append(f'  printf("{c} sizeof %zu\\n", sizeof({c}));')
+        for f in getattr(qcp, py)._fields_:
+            lines.append(f'  printf("{c} {f[0]} %zu\\n", offsetof({c}, {f[0]}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for ln in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        c, f, v = ln.split()
+        got[(c, f)] = int(v)
+    for py, c in STRUCTS:
+        cls = getattr(qcp, py)
+        assert got[(c, "sizeof")] == ctypes.sizeof(cls), c
+        for f in cls._fields_:
+            assert got[(c, f[0])] == getattr(cls, f[0]).offset, (c, f[0])
+    assert qcp.SERVE_BATCH_DTYPE.itemsize == ctypes.sizeof(qcp.ServeBatch)

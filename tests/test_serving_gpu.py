@@ -66,6 +66,25 @@ def test_admission_cap_on_result_bytes(served):
     assert largest > cap
 
 
+def test_serving_trace_records_every_run(served):
+    ix, objs, t, boxes, cls, want_offs, want_ids = served
+    stats, lat, _ = ix.serve(boxes, t, streams=3, max_batch=300, trace=100_000)
+    tr = stats["trace"]
+    assert len(tr) == stats["batches"]
+    assert int(tr["requests"].sum()) == len(boxes)
+    assert int(tr["hits"].sum()) == int(want_offs[-1])
+    assert set(np.unique(tr["worker"])) <= {0, 1, 2}
+    assert set(np.unique(tr["path"])) <= {0, 1, 2}
+    assert np.all(tr["requests"][tr["path"] == 0] <= 256)
+    for a, b in [("t_taken", "t_start"), ("t_start", "t_run"), ("t_run", "t_admitted"), ("t_admitted", "t_done")]:
+        assert np.all(tr[a] <= tr[b]), (a, b)
+    # a request's latency ends at its run's t_done
+    assert float(lat.max()) <= (float(tr["t_done"].max()) - float(t[0])) * 1e3 + 1.0
+    # a short trace keeps the first records and says how many runs there were
+    stats2, _, _ = ix.serve(boxes[:500], t[:500], streams=2, trace=3)
+    assert len(stats2["trace"]) == min(3, stats2["batches"])
+
+
 def test_serving_rejects_bad_trace(qcp, served):
     ix, objs, t, boxes, *_ = served
     bad = t[:10].copy()
