@@ -135,7 +135,7 @@ def algorithmic_bytes(st: dict, dims: int, fanout: int, is_rect: bool = False) -
 # DRAM bytes (read + write) per id of k_win_sort from an ncu capture of the
 # 16M-point Gaussian workload at 2,000 queries (profiles/k_win_sort_gauss16m_q2000.md),
 # applied to the ids of the timed launch: traffic grows with the ids processed.
-K_WIN_SORT_DRAM_BYTES_PER_ID = (851630848 + 797769216) / 211501325  # 7.80 B per id
+K_WIN_SORT_DRAM_BYTES_PER_ID = (848327424 + 801763584) / 211501325  # 7.80 B per id
 
 
 def load_workload(W, name, queries, world):
