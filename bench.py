@@ -275,18 +275,36 @@ def run_ours(args, rank, world, local):
 
     # ---- plain one-query-per-block traversal, same batch -------------------
     plain = None
+    forms = None
     if args.plain_steps > 0 and args.algo != "plain":
-        step_device("plain", False)
-        torch.cuda.synchronize()
-        e_a = torch.cuda.Event(enable_timing=True)
-        e_b = torch.cuda.Event(enable_timing=True)
-        e_a.record(stream)
-        for _ in range(args.plain_steps):
-            step_device("plain", False)
-        e_b.record(stream)
-        e_b.synchronize()
-        plain_ms = max_over_ranks(e_a.elapsed_time(e_b))
-        plain = world * Q * args.plain_steps / (plain_ms / 1e3)
+        def qps_of(fn):
+            fn()
+            torch.cuda.synchronize()
+            e_a = torch.cuda.Event(enable_timing=True)
+            e_b = torch.cuda.Event(enable_timing=True)
+            e_a.record(stream)
+            for _ in range(args.plain_steps):
+                fn()
+            e_b.record(stream)
+            e_b.synchronize()
+            return world * Q * args.plain_steps / (max_over_ranks(e_a.elapsed_time(e_b)) / 1e3)
+
+        def step_unsorted(algo):
+            r = ix.search(d_boxes, q=Q, algo=algo, sort=False, result_mem=qcp.MEM_DEVICE, stream=sp,
+                          blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"])
+            r.release()
+
+        plain = qps_of(lambda: step_device("plain", False))
+        # the same comparison at the output forms short of sorted ids: hit
+        # sets in traversal order, and per-query counts (the form the
+        # reference's plain kernel returns)
+        forms = {}
+        for form, fb, fp in [
+                ("unsorted_hit_sets", lambda: step_unsorted(args.algo), lambda: step_unsorted("plain")),
+                ("counts", lambda: ix.counts(d_boxes, q=Q, algo=args.algo, stream=sp),
+                 lambda: ix.counts(d_boxes, q=Q, algo="plain", stream=sp))]:
+            b_, p_ = qps_of(fb), qps_of(fp)
+            forms[form] = {"batched": round(b_, 1), "plain": round(p_, 1), "speedup": round(b_ / p_, 2)}
 
     # ---- e2e: host buffers through the public call -------------------------
     h_boxes = torch.from_numpy(boxes).pin_memory()
@@ -442,6 +460,12 @@ def run_ours(args, rank, world, local):
                        "host_build_s": round(build_s, 2),
                        "counts": "not compared: the kernel sums t_hit[0..255] but zeroes only [0..191] "
                                  "(mphr.cpp:325-328), so its counts carry leftover shared memory"}
+            ref_qps = Q / (ms / 1e3)
+            # batched against the reference's plain kernel: sorted ids (the
+            # full contract) and counts (the form that kernel returns)
+            ref_gpu["speedup_batched_sorted_ids"] = round(value / ref_qps, 1)
+            if forms:
+                ref_gpu["speedup_batched_counts"] = round(forms["counts"]["batched"] / ref_qps, 1)
 
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
     cpu = None
@@ -502,7 +526,8 @@ def run_ours(args, rank, world, local):
                      "algorithmic_bytes_per_launch": int(ab[dominant]),
                      "kernels_achieved_gbs": kernels_gbs},
         "plain": {"value": round(plain, 1) if plain else None, "unit": "queries/s",
-                  "speedup_batched_vs_plain": round(value / plain, 2) if plain else None},
+                  "speedup_batched_vs_plain": round(value / plain, 2) if plain else None,
+                  "by_output_form": forms},
         "e2e": {"value": round(e2e_value, 1), "unit": "queries/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": args.e2e_steps, "concurrent_calls": len(e2e_st)},
         "gpu_launches": int(launches),
