@@ -192,7 +192,7 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
 
     # ---- autotune on a separate query sample of the same distribution -------
-    knobs = {"fanout": args.fanout, "blocks_per_sm": 0, "win_bits": 0}
+    knobs = {"fanout": args.fanout, "blocks_per_sm": args.blocks_per_sm, "win_bits": args.win_bits}
     tune = None
     if args.algo == "batched" and not args.no_tune:
         sample = tune_sample(W, args.workload, w)
@@ -635,6 +635,8 @@ def main():
     ap.add_argument("--queries", type=int, default=None,
                     help="queries per GPU per step (default: the workload's own count; 10,000 for gauss16m)")
     ap.add_argument("--fanout", type=int, default=128)
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="traversal blocks per SM with --no-tune (0: default)")
+    ap.add_argument("--win-bits", type=int, default=0, help="sort window bits with --no-tune (0: default)")
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--e2e-streams", type=int, default=2,

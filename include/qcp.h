@@ -123,7 +123,7 @@ typedef struct qcp_query_opts {
   uint32_t flags;      /* QCP_QUERY_* bits */
   /* Tuning knobs (0 = default; qcp_autotune picks them): CUDA blocks per SM
    * of the batched traversal kernels (default 8, at most 32), and log2 of
-   * the id window of the per-query sort (default and largest 18, smallest
+   * the id window of the per-query sort (default 17, largest 18, smallest
    * 12; raised where the id range would need more than 8192 windows). */
   uint32_t blocks_per_sm;
   uint32_t win_bits;

@@ -554,7 +554,7 @@ static qcp_status run_query(qcp_index* ix, const float* boxes, uint32_t q, const
   qcp_status st = ws_reserve_queries(ix, ws, q);
   ws->timing = (o.flags & QCP_QUERY_TIMING) != 0;
   ws->blocks_per_sm = o.blocks_per_sm ? (o.blocks_per_sm > 32 ? 32u : o.blocks_per_sm) : 8u;
-  ws->win_bits = o.win_bits ? (o.win_bits < 12 ? 12u : o.win_bits) : 18u;
+  ws->win_bits = o.win_bits ? (o.win_bits < 12 ? 12u : o.win_bits) : kDefaultWinBits;
   ws->sort_small_jobs = ws->sort_msd_jobs = 0;
   ws->hybrid = o.algo == QCP_ALGO_HYBRID;
   ws->cpu_threads = o.cpu_threads;

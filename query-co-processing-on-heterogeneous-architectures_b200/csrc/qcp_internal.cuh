@@ -305,6 +305,8 @@ size_t sort_tables_bytes(const qcp_index* ix, const Workspace* ws, uint32_t q);
 void sort_window_shape(const qcp_index* ix, const Workspace* ws, uint32_t* wbits, uint32_t* G);
 // Largest window count whose per-window counts the write pass gathers.
 constexpr uint32_t kHistMaxG = 256;
+// Default log2 of the per-query sort's id windows (qcp_query_opts.win_bits).
+constexpr uint32_t kDefaultWinBits = 17;
 qcp_status ws_reserve_qwhist(Workspace* ws, size_t n);
 // Workspace construction and buffer reservation (qcp_capi.cu).
 qcp_status ws_reserve_queries(qcp_index* ix, Workspace* ws, uint32_t q);

@@ -78,7 +78,7 @@ extern "C" qcp_status qcp_plan_create(qcp_index* ix, uint32_t max_queries, uint6
   }
   Workspace* ws = p->ws;
   ws->blocks_per_sm = (opts && opts->blocks_per_sm) ? (opts->blocks_per_sm > 32 ? 32u : opts->blocks_per_sm) : 8u;
-  ws->win_bits = (opts && opts->win_bits) ? (opts->win_bits < 12 ? 12u : opts->win_bits) : 18u;
+  ws->win_bits = (opts && opts->win_bits) ? (opts->win_bits < 12 ? 12u : opts->win_bits) : kDefaultWinBits;
   qcp_status st = QCP_OK;
   do {
     const size_t row = 2 * (size_t)ix->dims;

@@ -45,16 +45,21 @@ constexpr uint32_t kTileThreads = 256;
 constexpr uint32_t kTileWarps = kTileThreads / 32;
 constexpr uint32_t kPerWarpMaxG = 256;  // per-warp window counters up to this G
 // ---- window sort ------------------------------------------------------------
-constexpr uint32_t kRankThreads = 512;
-constexpr uint32_t kRankWarps = kRankThreads / 32;
-constexpr uint32_t kBmWords = (1u << kWinBits) / 32;  // 8192
-constexpr uint32_t kLaneWords = kBmWords / kRankThreads;  // 16 words per thread in the enumeration
-constexpr uint32_t kRankBlocks = 3;                    // resident CTAs per SM
-constexpr uint32_t kStage = 6144;                      // staged output ids per window
-constexpr uint32_t kPrefetch = 4096;                   // ids of the next window loaded ahead
+// One instantiation per window size 2^BITS ids (BITS = 16, 17, 18): the
+// bitmap fills BITS-dependent shared memory, so smaller windows run more
+// CTAs per SM (3, 6, 12) at the same 48 warps; each thread owns 16 words.
+template <uint32_t BITS>
+struct WinCfg {
+  static constexpr uint32_t kWords = (1u << BITS) / 32;            // bitmap words
+  static constexpr uint32_t kThreads = kWords / 16;                // 512, 256, 128
+  static constexpr uint32_t kWarps = kThreads / 32;
+  static constexpr uint32_t kBlocks = 3u << (18 - BITS);           // resident CTAs per SM
+  static constexpr uint32_t kStage = BITS >= 18 ? 6144u : (BITS == 17 ? 3072u : 1408u);  // staged output ids
+  static constexpr uint32_t kPrefetch = 4096u >> (18 - BITS);      // ids of the next window loaded ahead
+};
+constexpr uint32_t kLaneWords = 16;                    // bitmap words per thread
 constexpr uint32_t kBatch = 8;                         // ids per thread per load round
 constexpr uint32_t kNone = 0xffffffffu;                // empty register slot
-static_assert(kLaneWords == 16, "k_win_sort reads a thread's words as four 16-byte groups");
 
 using Job = SortJob;
 
@@ -362,11 +367,12 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
 // ============================================================================
 // Window sort
 // ============================================================================
+template <uint32_t BITS>
 struct RankSmem {
-  uint32_t bm[kBmWords];        // one bit per possible id of the window
-  int32_t stage[kStage];        // output positions [0, kStage) of the window
-  int32_t pf[kPrefetch];        // first ids of the next window, loaded ahead
-  uint32_t wsum[kRankWarps];    // set bits in each warp's word range
+  uint32_t bm[WinCfg<BITS>::kWords];        // one bit per possible id of the window
+  int32_t stage[WinCfg<BITS>::kStage];      // output positions [0, kStage) of the window
+  int32_t pf[WinCfg<BITS>::kPrefetch];      // first ids of the next window, loaded ahead
+  uint32_t wsum[WinCfg<BITS>::kWarps];      // set bits in each warp's word range
 };
 
 // 4-byte global -> shared copies that run behind the CTA's other work
@@ -391,18 +397,23 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 //   3. the stage leaves in coalesced stores.
 // The ids of a window are distinct, so the set bits are the window's ids
 // and their enumeration in bit order is the window in ascending order.
-__global__ void __launch_bounds__(kRankThreads, kRankBlocks) k_win_sort(const uint32_t* __restrict__ njobs_p,
-                                                                        uint32_t G, uint32_t wbits,
-                                                                        const uint32_t* __restrict__ whist,
-                                                                        const unsigned long long* __restrict__ wbase,
-                                                                        const int32_t* __restrict__ src,
-                                                                        int32_t* __restrict__ out) {
+template <uint32_t BITS>
+__global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
+    k_win_sort(const uint32_t* __restrict__ njobs_p, uint32_t G, uint32_t wbits, const uint32_t* __restrict__ whist,
+               const unsigned long long* __restrict__ wbase, const int32_t* __restrict__ src,
+               int32_t* __restrict__ out) {
+  using C = WinCfg<BITS>;
+  constexpr uint32_t kRankThreads = C::kThreads;
+  constexpr uint32_t kRankWarps = C::kWarps;
+  constexpr uint32_t kBmWords = C::kWords;
+  constexpr uint32_t kStage = C::kStage;
+  constexpr uint32_t kPrefetch = C::kPrefetch;
   const uint32_t total = *njobs_p * G;  // (job, window) pairs
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  RankSmem& s = *reinterpret_cast<RankSmem*>(smem_raw);
+  RankSmem<BITS>& s = *reinterpret_cast<RankSmem<BITS>*>(smem_raw);
   const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   uint4* bm4 = reinterpret_cast<uint4*>(s.bm);
-  const uint32_t nwords = (1u << wbits) >> 5;   // wbits >= 12
+  const uint32_t nwords = (1u << wbits) >> 5;   // 12 <= wbits <= BITS
   const uint32_t tw0 = tid * kLaneWords;        // this thread's words [tw0, tw0 + kLaneWords)
   const bool owner = tw0 < nwords;
   // the four 16-byte groups of a thread's words are read starting at group
@@ -540,13 +551,37 @@ static uint32_t id_bits(uint64_t n) {
   return idbits;
 }
 
+// The window sort for 2^wbits-id windows (the instantiation whose bitmap
+// holds them), over at most `max_pairs` (job, window) pairs.
+template <uint32_t BITS>
+static void launch_win_sort_t(uint64_t max_pairs, uint32_t sms, const uint32_t* njobs, uint32_t G, uint32_t wbits,
+                              const uint32_t* whist, const unsigned long long* wbase, const int32_t* src,
+                              int32_t* out, cudaStream_t s) {
+  using C = WinCfg<BITS>;
+  const uint64_t cap = (uint64_t)sms * C::kBlocks;
+  const uint32_t grid = (uint32_t)(max_pairs < cap ? max_pairs : cap);
+  if (grid) k_win_sort<BITS><<<grid, C::kThreads, sizeof(RankSmem<BITS>), s>>>(njobs, G, wbits, whist, wbase, src, out);
+}
+
+static void launch_win_sort(uint64_t max_pairs, uint32_t sms, const uint32_t* njobs, uint32_t G, uint32_t wbits,
+                            const uint32_t* whist, const unsigned long long* wbase, const int32_t* src, int32_t* out,
+                            cudaStream_t s) {
+  if (wbits >= 18) launch_win_sort_t<18>(max_pairs, sms, njobs, G, wbits, whist, wbase, src, out, s);
+  else if (wbits == 17) launch_win_sort_t<17>(max_pairs, sms, njobs, G, wbits, whist, wbase, src, out, s);
+  else launch_win_sort_t<16>(max_pairs, sms, njobs, G, wbits, whist, wbase, src, out, s);
+}
+
 static qcp_status set_sort_attrs(const qcp_index* ix, size_t scatter_max) {
   static thread_local int attrs_device = -1;  // attributes are per device
   if (attrs_device != ix->device) {
     QCP_CUDA(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(BucketSmem)));
-    QCP_CUDA(cudaFuncSetAttribute(k_win_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sizeof(RankSmem)));
+    QCP_CUDA(cudaFuncSetAttribute(k_win_sort<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(RankSmem<16>)));
+    QCP_CUDA(cudaFuncSetAttribute(k_win_sort<17>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(RankSmem<17>)));
+    QCP_CUDA(cudaFuncSetAttribute(k_win_sort<18>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(RankSmem<18>)));
     QCP_CUDA(cudaFuncSetAttribute(k_win_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)scatter_max));
     attrs_device = ix->device;
@@ -602,13 +637,12 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   const uint32_t idbits = id_bits(ix->n);
   // window bits of this call: at most kWinBits (the bitmap), at least what
   // keeps the window count <= 8192 (the scatter's shared counters)
-  uint32_t wb = ws->win_bits ? ws->win_bits : kWinBits;
+  uint32_t wb = ws->win_bits ? ws->win_bits : kDefaultWinBits;
   if (wb > kWinBits) wb = kWinBits;
   if (idbits > 13 && wb < idbits - 13) wb = idbits - 13;
   const uint32_t wbits = idbits < wb ? idbits : wb;
   const uint32_t G = 1u << (idbits - wbits);
   const uint32_t sms = (uint32_t)num_sms();
-  const size_t rank_bytes = sizeof(RankSmem);
   const uint32_t nsets = (G <= kPerWarpMaxG) ? kTileWarps : 1u;
   const size_t scatter_bytes = (size_t)G * (8 + 4 + 4 * nsets) + kTile * 4;
 
@@ -657,9 +691,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
         big, map, tile_off, ctr + kCtrWork2, ws->out_ids, ws->tmp_ids, G, wbits, wcur);
     mark(ws, kEvSortPart, s);
     ws->sort_part_marked = ws->timing;
-    const uint32_t grid = (uint32_t)(nw < (uint64_t)sms * kRankBlocks ? nw : (uint64_t)sms * kRankBlocks);
-    k_win_sort<<<grid, kRankThreads, rank_bytes, s>>>(ctr + kCtrJobs1, G, wbits, whist, wbase, ws->tmp_ids,
-                                                      ws->out_ids);
+    launch_win_sort(nw, sms, ctr + kCtrJobs1, G, wbits, whist, wbase, ws->tmp_ids, ws->out_ids, s);
     note_launch(5);
     st = check_launch("segmented sort windows");
     // the tables go back to the pool below: make sure the kernels are done
@@ -675,7 +707,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
 void sort_window_shape(const qcp_index* ix, const Workspace* ws, uint32_t* wbits, uint32_t* G);
 static void window_shape(const qcp_index* ix, const Workspace* ws, uint32_t* wbits, uint32_t* G) {
   const uint32_t idbits = id_bits(ix->n);
-  uint32_t wb = ws->win_bits ? ws->win_bits : kWinBits;
+  uint32_t wb = ws->win_bits ? ws->win_bits : kDefaultWinBits;
   if (wb > kWinBits) wb = kWinBits;
   if (idbits > 13 && wb < idbits - 13) wb = idbits - 13;
   *wbits = idbits < wb ? idbits : wb;
@@ -739,8 +771,7 @@ qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void*
   k_win_scatter<<<sms * scatter_blocks_per_sm(scatter_bytes), kTileThreads, scatter_bytes, s>>>(
       big, ws->seg_hist, tile_off, ctr + kCtrWork2,
                                                              ws->out_ids, ws->tmp_ids, G, wbits, wcur);
-  k_win_sort<<<sms * kRankBlocks, kRankThreads, sizeof(RankSmem), s>>>(ctr + kCtrJobs1, G, wbits, whist, wbase,
-                                                             ws->tmp_ids, ws->out_ids);
+  launch_win_sort((uint64_t)-1, sms, ctr + kCtrJobs1, G, wbits, whist, wbase, ws->tmp_ids, ws->out_ids, s);
   note_launch(5);
   return check_launch("segmented sort (device counts)");
 }

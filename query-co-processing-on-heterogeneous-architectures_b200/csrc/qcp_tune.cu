@@ -99,7 +99,7 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
     };
     // 1. fan-out, default knobs
     const uint32_t fanouts[] = {64, 128, 256};
-    uint32_t best_f = 0, best_b = 8, best_w = 18;
+    uint32_t best_f = 0, best_b = 8, best_w = qcp::kDefaultWinBits;
     float best = 0.f, best_build = 0.f;
     for (uint32_t f : fanouts) {
       bo.fanout = f;
@@ -138,7 +138,9 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
       }
     }
     if (st != QCP_OK) break;
-    for (uint32_t w : {16u, 17u}) {
+    const uint32_t first_w = best_w;
+    for (uint32_t w : {16u, 17u, 18u}) {
+      if (w == first_w) continue;
       const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, best_b, w, repeats, e0, e1);
       if ((st = tr.st) != QCP_OK) break;
       record(best_f, best_b, w, tr.ms);

@@ -66,3 +66,15 @@ def test_plan_overflow_is_reported_and_plan_stays_usable(setup):
         assert np.array_equal(offs, want.offsets) and np.array_equal(ids, want.ids)
     with pytest.raises(qcp.QcpError):
         qcp.Plan(ix, 600, 5000).run_device(np.zeros((601, 6), np.float32))
+
+
+@pytest.mark.parametrize("wb", [16, 17])
+def test_plan_sorted_at_smaller_windows(setup, wb):
+    """Sorted plans at 2^16 / 2^17-id sort windows (their own window-sort
+    instantiations) return what qcp_query_batch returns."""
+    qcp, ix, objs, batches = setup
+    b = batches[0]
+    want = ix.search(b)
+    with qcp.Plan(ix, 600, 60_000_000, win_bits=wb) as plan:
+        offs, ids = plan.run(b)
+    assert np.array_equal(offs, want.offsets) and np.array_equal(ids, want.ids)
