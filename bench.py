@@ -135,7 +135,7 @@ def algorithmic_bytes(st: dict, dims: int, fanout: int, is_rect: bool = False) -
 # DRAM bytes (read + write) per id of k_win_sort from an ncu capture of the
 # 16M-point Gaussian workload at 2,000 queries (profiles/k_win_sort_gauss16m_q2000.md),
 # applied to the ids of the timed launch: traffic grows with the ids processed.
-K_WIN_SORT_DRAM_BYTES_PER_ID = (848327424 + 801763584) / 211501325  # 7.80 B per id
+K_WIN_SORT_DRAM_BYTES_PER_ID = (849777408 + 803374592) / 211501325  # 7.82 B per id
 
 
 def load_workload(W, name, queries, world):
@@ -328,10 +328,17 @@ def run_ours(args, rank, world, local):
     import concurrent.futures as cf
     e2e_st = [torch.cuda.Stream(dev) for _ in range(max(1, args.e2e_streams))]
     pool = cf.ThreadPoolExecutor(len(e2e_st))
-    # warm-up runs the calls concurrently too, so that every concurrent call
-    # has its own workspace and pinned result buffer sized before timing
-    for _ in range(max(1, args.warmup // 2)):
-        list(pool.map(lambda st_: step_host(st_), e2e_st))
+    # warm-up runs the calls concurrently too, all starting together (a
+    # barrier), so that every concurrent call has its own workspace and
+    # pinned result buffer sized before timing
+    import threading
+    start_together = threading.Barrier(len(e2e_st))
+
+    def warm(st_):
+        start_together.wait()
+        return step_host(st_)
+    for _ in range(max(2, args.warmup)):
+        list(pool.map(warm, e2e_st))
     barrier()
     torch.cuda.synchronize()
     e_a = torch.cuda.Event(enable_timing=True)
