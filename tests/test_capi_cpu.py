@@ -86,3 +86,29 @@ def test_binding_struct_layouts_match_header(qcp, tmp_path):
         for f in cls._fields_:
             assert got[(c, f[0])] == getattr(cls, f[0]).offset, (c, f[0])
     assert qcp.SERVE_BATCH_DTYPE.itemsize == ctypes.sizeof(qcp.ServeBatch)
+
+
+def test_newer_entry_points_reject_bad_arguments_without_device(qcp, tmp_path):
+    """Plans, serving, the autotuner, the no-allocation counts and index
+    files check their arguments before any device work: NULL handles and
+    empty inputs are BAD_ARG with a message, a missing index file is IO."""
+    lib = qcp.load_library()
+    P = ctypes.c_void_p
+    h = P()
+    BAD_ARG, IO = 1, 7
+    assert lib.qcp_plan_create(None, 16, 1000, None, ctypes.byref(h)) == BAD_ARG
+    assert lib.qcp_last_error()
+    assert lib.qcp_plan_run(None, None, 0, 0, None, None, None, None) == BAD_ARG
+    assert lib.qcp_plan_free(None) == 0
+    st = qcp.ServeStats()
+    assert lib.qcp_serve_replay(None, None, None, 0, None, None, ctypes.byref(st)) == BAD_ARG
+    assert lib.qcp_autotune(None, 0, 3, 0, None, 0, None, 0, None) == BAD_ARG
+    assert lib.qcp_query_counts_noalloc(None, None, 4, None, None) == BAD_ARG
+    buf = (ctypes.c_float * 12)()
+    res = qcp.Result()
+    assert lib.qcp_query_batch(None, buf, 2, None, ctypes.byref(res)) == BAD_ARG
+    assert lib.qcp_query_batch(None, buf, 2, None, None) == BAD_ARG
+    counts = (ctypes.c_uint64 * 2)()
+    assert lib.qcp_query_counts(None, buf, 2, None, counts) == BAD_ARG
+    assert lib.qcp_index_load(str(tmp_path / "none.qcpidx").encode(), None, ctypes.byref(h)) == IO
+    assert not h.value
