@@ -132,10 +132,78 @@ def algorithmic_bytes(st: dict, dims: int, fanout: int, is_rect: bool = False) -
             "sort_small": 8 * (hits - win), "sort_windows": 8 * win}
 
 
-# DRAM bytes (read + write) per id of k_win_sort from an ncu capture of the
-# 16M-point Gaussian workload at 2,000 queries (profiles/k_win_sort_gauss16m_q2000.md),
-# applied to the ids of the timed launch: traffic grows with the ids processed.
+# DRAM bytes (read + write) per id of k_win_sort measured by ncu on the
+# 16M-point Gaussian workload at 2,000 queries, applied to the ids of the
+# timed launch: traffic grows with the ids processed.
 K_WIN_SORT_DRAM_BYTES_PER_ID = (849777408 + 803374592) / 211501325  # 7.82 B per id
+
+KERNEL_NAMES = {"count": "k_leafscan<count>", "write": "k_leafscan<write>",
+                "sort_small": "k_sort_small", "sort_windows": "k_win_sort"}
+
+
+def roofline_of(stats, phase, steps, dims, fanout, is_rect, hbm, peak_kind):
+    """HBM roofline of the step's dominant kernel: algorithmic bytes of one
+    launch / that launch's CUDA-event time (the library's phase events on
+    the launching stream), against the measured copy bandwidth."""
+    ab = algorithmic_bytes(stats, dims, fanout, is_rect)
+    dominant = max(KERNEL_NAMES, key=lambda k: phase[k])
+    per_launch_ms = phase[dominant] / steps
+    achieved = ab[dominant] / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
+    traffic = None
+    if dominant == "sort_windows" and K_WIN_SORT_DRAM_BYTES_PER_ID:
+        traffic = int(K_WIN_SORT_DRAM_BYTES_PER_ID * stats["sort_window_ids"])
+    kernels_gbs = {KERNEL_NAMES[k]: round(ab[k] / (phase[k] / steps / 1e3) / 1e9, 1)
+                   for k in KERNEL_NAMES if phase[k] > 0}
+    return {"bound": "hbm", "kernel": KERNEL_NAMES[dominant],
+            "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(achieved / hbm, 4), "traffic": traffic,
+            "peak_kind": peak_kind, "launch_ms": round(per_launch_ms, 4),
+            "algorithmic_bytes_per_launch": int(ab[dominant]),
+            "kernels_achieved_gbs": kernels_gbs}
+
+
+class _DeviceArray:
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3}
+
+
+def verify_result(res, q, d_objs, d_boxes, dims, is_rect, chunk=1 << 24):
+    """Checks of every query's id list of a device-resident result, outside
+    any timed region: ids in [0, n), strictly ascending inside each slice,
+    and every id passes the closed-interval predicate !(q.lo > e.hi || q.hi <
+    e.lo) against its own box.  Returns (per-query counts, ids checked,
+    failure text or None).  With the counts equal to an independent count
+    (the reference's BVH traversal) every slice is the exact sorted hit set."""
+    import torch
+    offs = torch.as_tensor(_DeviceArray(res.offsets, q + 1, "<u8"), device=d_boxes.device).to(torch.int64)
+    total = int(res.total_hits)
+    counts = np.diff(offs.cpu().numpy()).astype(np.uint64)
+    if not total:
+        return counts, 0, None
+    ids = torch.as_tensor(_DeviceArray(res.ids, total, "<i4"), device=d_boxes.device)
+    n = d_objs.shape[0]
+    ends = offs[1:].contiguous()
+    for a in range(0, total, chunk):
+        b = min(total, a + chunk)
+        a0 = max(0, a - 1)
+        seg = ids[a0:b].to(torch.int64)
+        if int(seg.min()) < 0 or int(seg.max()) >= n:
+            return counts, a0, f"id out of range in [{a0}, {b})"
+        pos = torch.arange(a0, b, device=ids.device, dtype=torch.int64)
+        qi = torch.searchsorted(ends, pos, right=True)
+        bad_order = (seg[1:] <= seg[:-1]) & (qi[1:] == qi[:-1])
+        if bool(bad_order.any()):
+            return counts, a0, f"slice not ascending at position {int(torch.nonzero(bad_order)[0, 0]) + a0}"
+        box = d_boxes[qi]
+        e = d_objs[seg]
+        lo_e = e[:, :dims]
+        hi_e = e[:, dims:2 * dims] if is_rect else lo_e
+        bad = ((box[:, :dims] > hi_e) | (box[:, dims:] < lo_e)).any(1)
+        if bool(bad.any()):
+            k = int(torch.nonzero(bad)[0, 0])
+            return counts, a0, f"id {int(seg[k])} listed for query {int(qi[k])} fails the predicate"
+    return counts, total, None
 
 
 def load_workload(W, name, queries, world):
@@ -185,26 +253,26 @@ def run_ours(args, rank, world, local):
     boxes = np.ascontiguousarray(boxes_all[a:b])
     Q = boxes.shape[0]
 
-    d_objs = torch.from_numpy(w.objs).to(dev)
+    d_objs = torch.from_numpy(w.objs).to(dev)  # kept for the parity check
     d_boxes = torch.from_numpy(boxes).to(dev)
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
     torch.cuda.synchronize()
 
     # ---- autotune on a separate query sample of the same distribution -------
-    knobs = {"fanout": args.fanout, "blocks_per_sm": args.blocks_per_sm, "win_bits": args.win_bits}
+    knobs = {"fanout": args.fanout, "blocks_per_sm": args.blocks_per_sm, "win_bits": args.win_bits,
+             "leaf_prefetch": args.leaf_prefetch}
     tune = None
     if args.algo == "batched" and not args.no_tune:
         sample = tune_sample(W, args.workload, w)
         tune = qcp.autotune(w.objs, sample, is_rect=w.is_rect, dims=w.dims, repeats=2)
-        knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits")}
+        knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch")}
     args.fanout = knobs["fanout"]
 
     t0 = time.perf_counter()
     ix = qcp.Index.build(d_objs, dims=w.dims, n=w.n, is_rect=w.is_rect, fanout=args.fanout, stream=sp)
     build_ms = (time.perf_counter() - t0) * 1e3
     info = ix.info()
-    del d_objs
 
     def barrier():
         if world > 1:
@@ -219,7 +287,8 @@ def run_ours(args, rank, world, local):
 
     def step_device(algo, timing):
         r = ix.search(d_boxes, q=Q, algo=algo, result_mem=qcp.MEM_DEVICE, stream=sp, timing=timing,
-                      blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"])
+                      blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
+                    leaf_prefetch=knobs["leaf_prefetch"])
         hits = r.total_hits
         r.release()
         return hits
@@ -261,17 +330,17 @@ def run_ours(args, rank, world, local):
     # every candidate is ONE kernel launched once per step, timed by the
     # library's CUDA events on the launching stream
     hbm, peak_kind = peaks()
-    kernel_names = {"count": "k_leafscan<count>", "write": "k_leafscan<write>",
-                    "sort_small": "k_sort_small", "sort_windows": "k_win_sort"}
-    ab = algorithmic_bytes(stats, w.dims, args.fanout, w.is_rect)
-    dominant = max(kernel_names, key=lambda k: phase[k])
-    per_launch_ms = phase[dominant] / args.steps
-    achieved = ab[dominant] / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
-    traffic = None
-    if dominant == "sort_windows" and K_WIN_SORT_DRAM_BYTES_PER_ID:
-        traffic = int(K_WIN_SORT_DRAM_BYTES_PER_ID * stats["sort_window_ids"])
-    kernels_gbs = {kernel_names[k]: round(ab[k] / (phase[k] / args.steps / 1e3) / 1e9, 1)
-                   for k in kernel_names if phase[k] > 0}
+    roof = roofline_of(stats, phase, args.steps, w.dims, args.fanout, w.is_rect, hbm, peak_kind)
+
+    # ---- parity of the timed batch (after the timed region) -----------------
+    res = ix.search(d_boxes, q=Q, algo=args.algo, result_mem=qcp.MEM_DEVICE, stream=sp,
+                    blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
+                    leaf_prefetch=knobs["leaf_prefetch"])
+    got_counts, nchecked, fail = verify_result(res, Q, d_objs, d_boxes, w.dims, w.is_rect)
+    res.release()
+    parity = {"ids_checked": int(nchecked), "slices_ascending_and_in_box": fail is None}
+    if fail:
+        parity["failure"] = fail
 
     # ---- plain one-query-per-block traversal, same batch -------------------
     plain = None
@@ -291,7 +360,8 @@ def run_ours(args, rank, world, local):
 
         def step_unsorted(algo):
             r = ix.search(d_boxes, q=Q, algo=algo, sort=False, result_mem=qcp.MEM_DEVICE, stream=sp,
-                          blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"])
+                          blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
+                    leaf_prefetch=knobs["leaf_prefetch"])
             r.release()
 
         plain = qps_of(lambda: step_device("plain", False))
@@ -314,7 +384,8 @@ def run_ours(args, rank, world, local):
 
     def step_host(st):
         r = ix.search(h_np, algo=args.algo, result_mem=qcp.MEM_HOST, stream=st.cuda_stream, copy=False,
-                      blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"])
+                      blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
+                    leaf_prefetch=knobs["leaf_prefetch"])
         nb = (Q + 1) * 8 + r.total_hits * 4
         r.release()
         return nb
@@ -392,7 +463,7 @@ def run_ours(args, rank, world, local):
         plan_out = {}
         # (a) the timed batch itself through one plan
         with qcp.Plan(ix, Q, int(stats["hits"] * 1.05) + 1024, blocks_per_sm=knobs["blocks_per_sm"],
-                      win_bits=knobs["win_bits"]) as plan:
+                      win_bits=knobs["win_bits"], leaf_prefetch=knobs["leaf_prefetch"]) as plan:
             plan.run_device(d_boxes, q=Q, stream=sp)
             torch.cuda.synchronize()
             e_a = torch.cuda.Event(enable_timing=True)
@@ -443,7 +514,8 @@ def run_ours(args, rank, world, local):
             e_a.record(stream)
             for _ in range(args.steps):
                 ix.search(h_np, algo="hybrid", result_mem=qcp.MEM_DEVICE, stream=sp, handoff_level=h,
-                          blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"]).release()
+                          blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
+                    leaf_prefetch=knobs["leaf_prefetch"]).release()
             e_b.record(stream)
             e_b.synchronize()
             hm = e_a.elapsed_time(e_b) / args.steps
@@ -481,9 +553,26 @@ def run_ours(args, rank, world, local):
             cpu = {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
                    "sample": "unavailable: the reference's data path loads points only"}
         else:
-            cpu = cpu_baseline(w.objs, boxes, args.cpu_seconds, w.dims)
+            cpu, bvh_counts = cpu_baseline(w.objs, boxes, args.cpu_seconds, w.dims)
+            if bvh_counts is not None:
+                parity["counts_vs_reference_bvh"] = compare_counts(got_counts, bvh_counts)
+    if w.is_rect and args.plain_steps > 0:
+        # the reference has no rectangle loader: the plain traversal counts
+        parity["counts_vs_plain"] = compare_counts(got_counts, ix.counts(d_boxes, q=Q, algo="plain", stream=sp))
+    if world > 1:
+        bad = torch.tensor([0 if parity_ok(parity) else 1], device=dev)
+        dist.all_reduce(bad, op=dist.ReduceOp.MAX)
+        parity["all_ranks_ok"] = int(bad.item()) == 0
 
     ix.close()
+    del d_objs
+    torch.cuda.empty_cache()
+    others = None
+    if world == 1 and args.other_configs and args.workload == "gauss16m" and args.algo == "batched":
+        others = {}
+        for name in ("uniform2d64m", "rect8d32m"):
+            others[name] = measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind)
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -507,9 +596,13 @@ def run_ours(args, rank, world, local):
             "workload": f"{w.name}: {w.n} {w.dims}-D {'rectangles' if w.is_rect else 'points'}, "
                         f"{Q} queries per GPU per step",
             "fanout": args.fanout, "blocks_per_sm": knobs["blocks_per_sm"] or 8,
-            "win_bits": knobs["win_bits"] or 18,
+            "win_bits": knobs["win_bits"] or 17,
+            "leaf_prefetch": knobs["leaf_prefetch"] or 2,
             "tuned": None if tune is None else {"sample_queries": 2000, "best_ms": round(tune["best_ms"], 3),
+                                                "trial_fields": ["fanout", "blocks_per_sm", "win_bits",
+                                                                 "leaf_prefetch", "ms"],
                                                 "trials": [[t["fanout"], t["blocks_per_sm"], t["win_bits"],
+                                                            t["leaf_prefetch"],
                                                             round(t["ms"], 3)] for t in tune["trials"]]},
             "algo": args.algo, "queries_per_step_per_gpu": Q,
             "n_objects": w.n, "key": f"hilbert {info['key_bits']} bits/dim",
@@ -526,12 +619,8 @@ def run_ours(args, rank, world, local):
         "work_per_step": {k: stats[k] for k in ["leaf_items", "leaves_covered", "leaves_partial",
                                                  "objects_covered", "sort_small_jobs", "sort_msd_jobs",
                                                  "sort_window_ids"]},
-        "roofline": {"bound": "hbm", "kernel": kernel_names[dominant],
-                     "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                     "frac": round(achieved / hbm, 4), "traffic": traffic,
-                     "peak_kind": peak_kind, "launch_ms": round(per_launch_ms, 4),
-                     "algorithmic_bytes_per_launch": int(ab[dominant]),
-                     "kernels_achieved_gbs": kernels_gbs},
+        "roofline": roof,
+        "parity": parity,
         "plain": {"value": round(plain, 1) if plain else None, "unit": "queries/s",
                   "speedup_batched_vs_plain": round(value / plain, 2) if plain else None,
                   "by_output_form": forms},
@@ -550,7 +639,141 @@ def run_ours(args, rank, world, local):
         out["hybrid"] = hybrid
     if cpu is not None:
         out["cpu_baseline"] = cpu
+    if others is not None:
+        out["other_configs"] = others
     print(json.dumps(out), flush=True)
+    ok = parity_ok(parity) and all(parity_ok(o.get("parity", {})) for o in (others or {}).values())
+    if not ok:
+        print("bench: PARITY FAILED (see the parity keys of the line above)", file=sys.stderr, flush=True)
+        sys.exit(3)
+
+
+def measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind):
+    """A compact line for another workload on the same GPU: tuned knobs,
+    device-resident queries/s, the plain traversal, host-buffer e2e, the
+    build, the dominant kernel's roofline and the parity of the batch."""
+    import torch
+    w, boxes = load_workload(W, name, None, 1)
+    Q = len(boxes)
+    stream = torch.cuda.current_stream(dev)
+    d_objs = torch.from_numpy(w.objs).to(dev)
+    d_boxes = torch.from_numpy(boxes).to(dev)
+    knobs = {"fanout": 128, "blocks_per_sm": 0, "win_bits": 0, "leaf_prefetch": 0}
+    tune = None
+    if not args.no_tune:
+        tune = qcp.autotune(w.objs, tune_sample(W, name, w), is_rect=w.is_rect, dims=w.dims, repeats=2)
+        knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch")}
+    build = dict(fanout=knobs["fanout"], dims=w.dims, n=w.n, is_rect=w.is_rect, key_bits=w.key_bits, stream=sp)
+    qcp.Index.build(d_objs, **build).close()  # warm-up build
+    torch.cuda.synchronize()
+    build_ms = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        ixb = qcp.Index.build(d_objs, **build)
+        build_ms.append((time.perf_counter() - t0) * 1e3)
+        ixb.close()
+    ix = qcp.Index.build(d_objs, **build)
+    info = ix.info()
+    kq = dict(blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
+                    leaf_prefetch=knobs["leaf_prefetch"])
+
+    def step(algo, timing=False):
+        r = ix.search(d_boxes, q=Q, algo=algo, result_mem=qcp.MEM_DEVICE, stream=sp, timing=timing, **kq)
+        r.release()
+
+    def timed(algo, steps, timing=False):
+        for _ in range(args.warmup):
+            step(algo, timing)
+        torch.cuda.synchronize()
+        e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        phase = {"expand": 0.0, "count": 0.0, "scan": 0.0, "write": 0.0, "sort": 0.0, "total": 0.0,
+                 "sort_small": 0.0, "sort_partition": 0.0, "sort_windows": 0.0}
+        e_a.record(stream)
+        st = None
+        for _ in range(steps):
+            step(algo, timing)
+            if timing:
+                st = qcp.last_stats()
+                for k in phase:
+                    phase[k] += st[f"ms_{k}"]
+        e_b.record(stream)
+        e_b.synchronize()
+        return e_a.elapsed_time(e_b), phase, st
+
+    with ClockSampler(dev.index or 0) as clocks:
+        ms, phase, stats = timed("batched", args.steps, timing=True)
+    clk = clocks.summary()
+    value = Q * args.steps / (ms / 1e3)
+    roof = roofline_of(stats, phase, args.steps, w.dims, knobs["fanout"], w.is_rect, hbm, peak_kind)
+    plain = None
+    if args.plain_steps > 0:
+        pms, _, _ = timed("plain", args.plain_steps)
+        plain = Q * args.plain_steps / (pms / 1e3)
+    # e2e through the public call with pinned host boxes and host hit lists
+    h_np = torch.from_numpy(boxes).pin_memory().numpy()
+    for _ in range(2):
+        ix.search(h_np, result_mem=qcp.MEM_HOST, stream=sp, copy=False, **kq).release()
+    torch.cuda.synchronize()
+    e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_a.record(stream)
+    d2h = 0
+    for _ in range(args.e2e_steps):
+        r = ix.search(h_np, result_mem=qcp.MEM_HOST, stream=sp, copy=False, **kq)
+        d2h = (Q + 1) * 8 + r.total_hits * 4
+        r.release()
+    e_b.record(stream)
+    e_b.synchronize()
+    e2e = Q * args.e2e_steps / (e_a.elapsed_time(e_b) / 1e3)
+    # parity of the batch
+    res = ix.search(d_boxes, q=Q, result_mem=qcp.MEM_DEVICE, stream=sp, **kq)
+    got, nchecked, fail = verify_result(res, Q, d_objs, d_boxes, w.dims, w.is_rect)
+    res.release()
+    parity = {"ids_checked": int(nchecked), "slices_ascending_and_in_box": fail is None}
+    if fail:
+        parity["failure"] = fail
+    if w.is_rect:
+        parity["counts_vs_plain"] = compare_counts(got, ix.counts(d_boxes, q=Q, algo="plain", stream=sp))
+        cpu = None
+    else:
+        cpu, want = cpu_baseline(w.objs, boxes, 0.0 if args.no_cpu_baseline else args.cpu_seconds / 3, w.dims)
+        if want is not None:
+            parity["counts_vs_reference_bvh"] = compare_counts(got, want)
+    ix.close()
+    del d_objs, d_boxes
+    torch.cuda.empty_cache()
+    out = {"workload": f"{w.name}: {w.n} {w.dims}-D {'rectangles' if w.is_rect else 'points'}, {Q} queries per step",
+           "value": round(value, 1), "unit": "queries/s", "ms_per_step": round(ms / args.steps, 4),
+           "steps": args.steps, "warmup": args.warmup, "hits_per_step": int(stats["hits"]),
+           "knobs": knobs, "key": f"hilbert {info['key_bits']} bits/dim", "levels": info["levels"],
+           "tuned": None if tune is None else [[t["fanout"], t["blocks_per_sm"], t["win_bits"], t["leaf_prefetch"],
+                                                round(t["ms"], 3)]
+                                               for t in tune["trials"]],
+           "phase_ms_per_step": {k: round(v / args.steps, 4) for k, v in phase.items()},
+           "roofline": roof,
+           "plain": {"value": round(plain, 1) if plain else None,
+                     "speedup_batched_vs_plain": round(value / plain, 2) if plain else None},
+           "e2e": {"value": round(e2e, 1), "unit": "queries/s", "h2d_bytes_per_step": int(boxes.nbytes),
+                   "d2h_bytes_per_step": int(d2h)},
+           "build_ms": {"min": round(min(build_ms), 2), "runs": [round(x, 2) for x in build_ms],
+                        "what": "qcp_index_build from device-resident objects, host wall clock, allocation included"},
+           "parity": parity, "clocks": clk}
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
+    return out
+
+
+def compare_counts(got, want):
+    got = np.asarray(got, dtype=np.uint64)
+    want = np.asarray(want, dtype=np.uint64)
+    bad = np.nonzero(got != want)[0]
+    return {"queries": int(len(want)), "equal": bool(len(bad) == 0 and len(got) == len(want)),
+            "mismatches": int(len(bad)), "first_mismatch": int(bad[0]) if len(bad) else None}
+
+
+def parity_ok(p: dict) -> bool:
+    if p.get("slices_ascending_and_in_box") is False or p.get("all_ranks_ok") is False:
+        return False
+    return all(v.get("equal", True) for k, v in p.items() if k.startswith("counts_vs"))
 
 
 def _reference_lib(dims: int = 3):
@@ -561,26 +784,32 @@ def _reference_lib(dims: int = 3):
     return Reference(dims)
 
 
-def cpu_baseline(objs, boxes, seconds, dims=3):
+def cpu_baseline(objs, boxes, seconds, dims=3, counts=True):
     """The reference's CPU BVH traversal on this host's cores over a bounded
-    sample of the batch (as many queries as fit in about `seconds`)."""
+    sample of the batch (as many queries as fit in about `seconds`), and
+    (counts=True) the reference BVH's per-query counts of the whole batch
+    (BVH::TraverseInternalNodes, src/tree/bvh.cpp:256-278) for the parity
+    check.  Returns (baseline dict, counts or None)."""
     ref = _reference_lib(dims)
     if ref is None:
-        return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
-                "sample": "unavailable: oracle/_ref not built"}
+        return ({"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
+                 "sample": "unavailable: oracle/_ref not built"}, None)
     threads = os.cpu_count() or 1
     h = ref.bvh_build(objs)
+    want = None
     try:
         n = min(len(boxes), 256)
         t = ref.bvh_search_seconds(h, boxes[:n], threads)
-        while t < seconds / 4 and n < len(boxes):
+        while seconds > 0 and t < seconds / 4 and n < len(boxes):
             n = min(len(boxes), int(n * max(2.0, seconds / max(t, 1e-3) / 2)))
             t = ref.bvh_search_seconds(h, boxes[:n], threads)
+        if counts:
+            want = ref.bvh_counts(h, boxes, threads)
     finally:
         ref.bvh_free(h)
-    return {"value": round(n / t, 1), "unit": "queries/s", "cores": threads, "kind": "reference",
-            "sample": f"first {n} of the {len(boxes)} queries of one step, {t:.2f} s, "
-                      f"BVH::Search with {threads} threads"}
+    return ({"value": round(n / t, 1), "unit": "queries/s", "cores": threads, "kind": "reference",
+             "sample": f"first {n} of the {len(boxes)} queries of one step, {t:.2f} s, "
+                       f"BVH::Search with {threads} threads"}, want)
 
 
 def run_reference(args, rank, world):
@@ -644,6 +873,8 @@ def main():
     ap.add_argument("--fanout", type=int, default=128)
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="traversal blocks per SM with --no-tune (0: default)")
     ap.add_argument("--win-bits", type=int, default=0, help="sort window bits with --no-tune (0: default)")
+    ap.add_argument("--leaf-prefetch", type=int, default=0,
+                    help="leaf prefetch buffers per warp with --no-tune (0: default 2, 1: none)")
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--e2e-streams", type=int, default=2,
@@ -659,6 +890,8 @@ def main():
                     help="length of the serving replay at N=1 (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=200_000.0, help="serving arrivals per second")
     ap.add_argument("--serve-streams", type=int, default=4, help="serving batches in flight")
+    ap.add_argument("--no-other-configs", dest="other_configs", action="store_false",
+                    help="skip the compact lines of the 64M 2-D and 32M 8-D rectangle workloads")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

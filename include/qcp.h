@@ -132,6 +132,13 @@ typedef struct qcp_query_opts {
    * the root's level = everything on the GPU). */
   uint32_t cpu_threads;
   uint32_t handoff_level;
+  /* Leaf prefetch of the batched traversal (0 = default): partially covered
+   * leaves are copied into a per-warp shared-memory ring by bulk copies
+   * (cp.async.bulk on the TMA unit) this many leaves ahead of the one being
+   * tested; 0 = 2 buffers, 1 = no ring (every lane loads its coordinates
+   * itself), 2..4 = that many buffers (fewer where shared memory is short).
+   * qcp_autotune picks it. */
+  uint32_t leaf_prefetch;
 } qcp_query_opts;
 
 /* flags: record CUDA events around every phase of the call; the times are
@@ -206,28 +213,56 @@ qcp_status qcp_index_load(const char* path, void* stream, qcp_index** out);
 qcp_status qcp_index_export(const qcp_index* index, uint64_t* keys, int32_t* ids,
                             uint32_t level, float* mbr);
 
+/* Captured build: the device bulk load of n objects of one shape (dims,
+ * is_rect, fan-out, key mode and bits from opts; QCP_KEY_NORM or
+ * QCP_KEY_REF) recorded once into a CUDA graph -- Hilbert keys, the 64-bit
+ * radix sort, packing into the SoA leaf layout and the bottom-up MBR levels
+ * -- over buffers the plan owns, and replayed by qcp_build_plan_run with no
+ * allocation and no host round trip between the steps.  The plan owns the
+ * index it builds: qcp_build_plan_run sets *index to it (valid until the
+ * next run or qcp_build_plan_free; queries on it work as on any index, and a
+ * run must not overlap queries on it).  objs: n rows as for qcp_index_build
+ * in host or device memory (objs_mem), copied into the plan's input buffer,
+ * or NULL when the caller has written them into qcp_build_plan_input(plan)
+ * itself.  Non-finite coordinates fail the run with QCP_ERR_BAD_ARG.
+ * Replaces the reference's host build and its copy of the tree to the device
+ * (Tree::Bottom_Up, src/tree/tree.cpp:410-495; MPHR::Build,
+ * src/tree/mphr.cpp:60-133). */
+typedef struct qcp_build_plan qcp_build_plan;
+
+qcp_status qcp_build_plan_create(uint64_t n, uint32_t dims, uint32_t is_rect, const qcp_build_opts* opts,
+                                 qcp_build_plan** plan);
+float* qcp_build_plan_input(qcp_build_plan* plan);
+qcp_status qcp_build_plan_run(qcp_build_plan* plan, const float* objs, uint32_t objs_mem, void* stream,
+                              qcp_index** index);
+qcp_status qcp_build_plan_free(qcp_build_plan* plan);
+
 /* Hit count of each of q (<= 262144) queries, computed by the batched
  * traversal, without allocating any memory -- for callers that must not call
  * cudaMalloc while they query (device memory owned by another allocator,
  * serving loops that cannot take cudaMalloc's implicit synchronisation,
  * allocation only at start-up by policy).  d_boxes (q rows of 2*dims floats)
- * and d_counts (q entries) are device memory the caller owns.  The
- * traversal's scratch is one fixed array of about 20 MiB in the library's
- * device image, held by every GPU that loads the library until exit and
- * shared by all calls: calls that overlap on the GPU race and must be
- * serialised by the caller.  The first call on a device looks up the
- * array's device address; make it before any stream capture.  A batch whose
- * traversal frontier exceeds the scratch returns QCP_ERR_OUTPUT_OVERFLOW
- * (split the batch).  No counterpart in the reference. */
+ * and d_counts (q entries) are device memory the caller owns, on the
+ * index's device (or managed memory); device memory of another GPU is
+ * refused with QCP_ERR_BAD_ARG.  The traversal's scratch is one fixed array
+ * of about 20 MiB in the library's device image, held by every GPU that
+ * loads the library until exit and shared by all calls: calls that overlap
+ * on the GPU race and must be serialised by the caller.  The first call on a
+ * device looks up the array's device address and keeps it for the life of
+ * the process; make it before any stream capture.  A cudaDeviceReset after
+ * that first call is not supported (it invalidates every index as well).  A
+ * batch whose traversal frontier exceeds the scratch's 2^20 (query, node)
+ * items returns QCP_ERR_OUTPUT_OVERFLOW (split the batch); d_counts is then
+ * undefined.  No counterpart in the reference. */
 qcp_status qcp_query_counts_noalloc(qcp_index* index, const float* d_boxes, uint32_t q,
                                     uint64_t* d_counts, void* stream);
 
 /* Autotuner: picks the build fan-out and the query knobs (blocks_per_sm,
- * win_bits) for a data set and a sample of its queries by timing trials on
- * the current device: every fan-out in {64, 128, 256} is built and queried
- * with the default knobs, then blocks_per_sm in {4, 8, 16} and win_bits in
- * {16, 17, 18} are tried one after the other at the best fan-out (coordinate
- * descent); each trial is the median of `repeats` timed batches of the
+ * win_bits, leaf_prefetch) for a data set and a sample of its queries by
+ * timing trials on the current device: every fan-out in {64, 128, 256} is
+ * built and queried with the default knobs, then blocks_per_sm in {4, 8,
+ * 16}, win_bits in {16, 17, 18} and leaf_prefetch in {1, 2, 3} are tried one
+ * after the other at the best fan-out (coordinate descent); each trial is the median of `repeats` timed batches of the
  * sample (sorted output) after one untimed batch.  objs and boxes are host
  * memory as for qcp_index_build / qcp_query_batch; `base` supplies the key
  * mode, key bits and stream (its fanout is ignored).  The reference fixes
@@ -245,6 +280,8 @@ typedef struct qcp_tune_result {
   uint32_t trial_blocks_per_sm[QCP_TUNE_MAX_TRIALS];
   uint32_t trial_win_bits[QCP_TUNE_MAX_TRIALS];
   float trial_ms[QCP_TUNE_MAX_TRIALS];
+  uint32_t leaf_prefetch;     /* best qcp_query_opts.leaf_prefetch */
+  uint32_t trial_leaf_prefetch[QCP_TUNE_MAX_TRIALS];
 } qcp_tune_result;
 
 qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims, uint32_t is_rect, const float* boxes,
@@ -257,7 +294,7 @@ qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims, uint32_t i
  * creation (device memory for max_queries boxes, the frontier, max_hits ids
  * twice, the sort's tables) so every phase runs from device-resident counts,
  * and one graph launch replaces its ~20 kernel launches and 3 host round
- * trips.  opts: blocks_per_sm, win_bits and unsorted are used (algo must be
+ * trips.  opts: blocks_per_sm, win_bits, leaf_prefetch and unsorted are used (algo must be
  * batched; NULL = defaults).  qcp_plan_create runs the pipeline once on an
  * empty batch before capturing it.
  *

@@ -57,7 +57,8 @@ class QueryOpts(ctypes.Structure):
                 ("result_mem", ctypes.c_uint32), ("unsorted", ctypes.c_uint32),
                 ("stream", ctypes.c_void_p), ("flags", ctypes.c_uint32),
                 ("blocks_per_sm", ctypes.c_uint32), ("win_bits", ctypes.c_uint32),
-                ("cpu_threads", ctypes.c_uint32), ("handoff_level", ctypes.c_uint32)]
+                ("cpu_threads", ctypes.c_uint32), ("handoff_level", ctypes.c_uint32),
+                ("leaf_prefetch", ctypes.c_uint32)]
 
 
 QUERY_TIMING = 1
@@ -117,7 +118,9 @@ class TuneResult(ctypes.Structure):
                 ("trial_fanout", ctypes.c_uint32 * TUNE_MAX_TRIALS),
                 ("trial_blocks_per_sm", ctypes.c_uint32 * TUNE_MAX_TRIALS),
                 ("trial_win_bits", ctypes.c_uint32 * TUNE_MAX_TRIALS),
-                ("trial_ms", ctypes.c_float * TUNE_MAX_TRIALS)]
+                ("trial_ms", ctypes.c_float * TUNE_MAX_TRIALS),
+                ("leaf_prefetch", ctypes.c_uint32),
+                ("trial_leaf_prefetch", ctypes.c_uint32 * TUNE_MAX_TRIALS)]
 
 
 class Result(ctypes.Structure):
@@ -162,6 +165,10 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
         "qcp_plan_run": ([P, P, U32, U32, P, ctypes.POINTER(U64), ctypes.POINTER(P), ctypes.POINTER(P)],
                          ctypes.c_int),
         "qcp_plan_free": ([P], ctypes.c_int),
+        "qcp_build_plan_create": ([U64, U32, U32, ctypes.POINTER(BuildOpts), ctypes.POINTER(P)], ctypes.c_int),
+        "qcp_build_plan_input": ([P], P),
+        "qcp_build_plan_run": ([P, P, U32, P, ctypes.POINTER(P)], ctypes.c_int),
+        "qcp_build_plan_free": ([P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -217,10 +224,11 @@ class SearchResult:
 class Index:
     """A device-resident bulk-loaded R-tree (one GPU)."""
 
-    def __init__(self, handle: ctypes.c_void_p, dims: int, is_rect: bool):
+    def __init__(self, handle: ctypes.c_void_p, dims: int, is_rect: bool, owned: bool = True):
         self._h = handle
         self.dims = dims
         self.is_rect = is_rect
+        self._owned = owned  # False: a BuildPlan's index, freed with the plan
 
     # -- construction ---------------------------------------------------------
     @classmethod
@@ -267,9 +275,9 @@ class Index:
         _check(load_library().qcp_index_save(self._h, str(path).encode()))
 
     def close(self) -> None:
-        if self._h:
+        if self._h and self._owned:
             load_library().qcp_index_free(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:
@@ -309,15 +317,16 @@ class Index:
 
     # -- queries --------------------------------------------------------------
     def _opts(self, algo, boxes_mem, result_mem, sort, stream, timing=False, blocks_per_sm=0, win_bits=0,
-              cpu_threads=0, handoff_level=0):
+              cpu_threads=0, handoff_level=0, leaf_prefetch=0):
         a = {"batched": ALGO_BATCHED, "plain": ALGO_PLAIN, "hybrid": ALGO_HYBRID}.get(algo, algo)
         return QueryOpts(a, boxes_mem, result_mem, 0 if sort else 1, ctypes.c_void_p(stream or None),
-                         QUERY_TIMING if timing else 0, blocks_per_sm, win_bits, cpu_threads, handoff_level)
+                         QUERY_TIMING if timing else 0, blocks_per_sm, win_bits, cpu_threads, handoff_level,
+                         leaf_prefetch)
 
     def search(self, boxes, algo="batched", sort: bool = True, result_mem: int = MEM_HOST,
                q: int | None = None, stream: int = 0, timing: bool = False,
                copy: bool = True, blocks_per_sm: int = 0, win_bits: int = 0, cpu_threads: int = 0,
-               handoff_level: int = 0) -> SearchResult:
+               handoff_level: int = 0, leaf_prefetch: int = 0) -> SearchResult:
         """Run a batch of box queries.  Host numpy boxes (q x 2D) or a CUDA
         tensor/pointer (then pass q).  Host results are copied into numpy
         arrays (copy=False: numpy views of the library's pinned result arena,
@@ -332,7 +341,7 @@ class Index:
                 raise ValueError("device boxes need q")
             b, nq, ptr, bmem = boxes, q, ctypes.c_void_p(_device_ptr(boxes)), MEM_DEVICE
         opts = self._opts(algo, bmem, result_mem, sort, stream, timing, blocks_per_sm, win_bits, cpu_threads,
-                          handoff_level)
+                          handoff_level, leaf_prefetch)
         r = Result()
         _check(lib.qcp_query_batch(self._h, ptr, nq, ctypes.byref(opts), ctypes.byref(r)))
         if result_mem == MEM_HOST and not copy:
@@ -357,7 +366,8 @@ class Index:
             return SearchResult(offs, ids, total, MEM_HOST)
         return SearchResult(r.offsets, r.ids, int(r.total_hits), MEM_DEVICE, raw=r)
 
-    def counts(self, boxes, algo="batched", q: int | None = None, stream: int = 0) -> np.ndarray:
+    def counts(self, boxes, algo="batched", q: int | None = None, stream: int = 0,
+               leaf_prefetch: int = 0) -> np.ndarray:
         lib = load_library()
         if isinstance(boxes, np.ndarray):
             b = np.ascontiguousarray(boxes, dtype=np.float32).reshape(-1, 2 * self.dims)
@@ -365,7 +375,7 @@ class Index:
         else:
             b, nq, ptr, bmem = boxes, q, ctypes.c_void_p(_device_ptr(boxes)), MEM_DEVICE
         out = np.zeros(nq, np.uint64)
-        opts = self._opts(algo, bmem, MEM_HOST, True, stream)
+        opts = self._opts(algo, bmem, MEM_HOST, True, stream, leaf_prefetch=leaf_prefetch)
         _check(lib.qcp_query_counts(self._h, ptr, nq, ctypes.byref(opts), _ptr(out)))
         return out
 
@@ -423,10 +433,11 @@ class Plan:
     offsets and ids; run_device() the plan's device pointers."""
 
     def __init__(self, index: "Index", max_queries: int, max_hits: int, sort: bool = True,
-                 blocks_per_sm: int = 0, win_bits: int = 0):
+                 blocks_per_sm: int = 0, win_bits: int = 0, leaf_prefetch: int = 0):
         self.index = index
         self._h = ctypes.c_void_p()
-        opts = index._opts("batched", MEM_HOST, MEM_DEVICE, sort, 0, False, blocks_per_sm, win_bits)
+        opts = index._opts("batched", MEM_HOST, MEM_DEVICE, sort, 0, False, blocks_per_sm, win_bits,
+                           leaf_prefetch=leaf_prefetch)
         _check(load_library().qcp_plan_create(index._h, max_queries, max_hits, ctypes.byref(opts),
                                               ctypes.byref(self._h)))
 
@@ -463,6 +474,53 @@ class Plan:
         self.close()
 
 
+class BuildPlan:
+    """A captured device build for n objects of one shape
+    (qcp_build_plan_create): run() rebuilds the plan's index from new
+    objects by one graph launch and returns it (valid until the next run
+    or close; do not close it yourself)."""
+
+    def __init__(self, n: int, dims: int, is_rect: bool = False, fanout: int = 128, key_mode: int = KEY_NORM,
+                 key_bits: int = 0):
+        self.n, self.dims, self.is_rect = n, dims, is_rect
+        self._h = ctypes.c_void_p()
+        opts = BuildOpts(fanout, key_mode, key_bits, MEM_HOST, None, 0, 0)
+        _check(load_library().qcp_build_plan_create(n, dims, 1 if is_rect else 0, ctypes.byref(opts),
+                                                    ctypes.byref(self._h)))
+
+    def input_ptr(self) -> int:
+        """Device address of the plan's input buffer (n rows of D or 2D floats)."""
+        return int(load_library().qcp_build_plan_input(self._h) or 0)
+
+    def run(self, objs=None, stream: int = 0) -> Index:
+        """objs: a host numpy array, a CUDA tensor / device pointer, or None
+        when the objects are already in input_ptr()."""
+        lib = load_library()
+        h = ctypes.c_void_p()
+        if objs is None:
+            ptr, mem = None, MEM_DEVICE
+        elif isinstance(objs, np.ndarray):
+            a = np.ascontiguousarray(objs, dtype=np.float32)
+            if a.shape[0] != self.n:
+                raise ValueError("the plan was created for a different object count")
+            ptr, mem = _ptr(a), MEM_HOST
+        else:
+            ptr, mem = ctypes.c_void_p(_device_ptr(objs)), MEM_DEVICE
+        _check(lib.qcp_build_plan_run(self._h, ptr, mem, ctypes.c_void_p(stream or None), ctypes.byref(h)))
+        return Index(h, self.dims, self.is_rect, owned=False)
+
+    def close(self) -> None:
+        if self._h:
+            load_library().qcp_build_plan_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def autotune(objs, boxes, is_rect: bool = False, dims: int | None = None, key_mode: int = 0,
              repeats: int = 3) -> dict:
     """Pick the fan-out and the query knobs (blocks_per_sm, win_bits) for a
@@ -478,9 +536,10 @@ def autotune(objs, boxes, is_rect: bool = False, dims: int | None = None, key_mo
                                        ctypes.byref(bo), repeats, ctypes.byref(r)))
     n = r.trials
     return {"fanout": r.fanout, "blocks_per_sm": r.blocks_per_sm, "win_bits": r.win_bits,
-            "best_ms": r.best_ms, "build_ms": r.build_ms,
+            "leaf_prefetch": r.leaf_prefetch, "best_ms": r.best_ms, "build_ms": r.build_ms,
             "trials": [{"fanout": r.trial_fanout[i], "blocks_per_sm": r.trial_blocks_per_sm[i],
-                        "win_bits": r.trial_win_bits[i], "ms": r.trial_ms[i]} for i in range(n)]}
+                        "win_bits": r.trial_win_bits[i], "leaf_prefetch": r.trial_leaf_prefetch[i],
+                        "ms": r.trial_ms[i]} for i in range(n)]}
 
 
 def last_stats() -> dict:

@@ -21,6 +21,7 @@
 #include <mutex>
 
 #include "qcp_internal.cuh"
+#include "qcp_tree.cuh"
 
 namespace qcp {
 
@@ -39,19 +40,22 @@ __device__ __forceinline__ int64_t quantise(float p, uint32_t bits, uint32_t mod
   return (int64_t)(q > maxq ? maxq : q);
 }
 
-__global__ void k_keys(const float* __restrict__ objs, uint64_t n, uint32_t dims, uint32_t is_rect,
-                       uint32_t mode, uint32_t bits, uint64_t* __restrict__ keys,
-                       uint32_t* __restrict__ vals) {
-  const uint32_t stride = is_rect ? 2 * dims : dims;
+// One thread per object, the dimension count a template parameter so that
+// the coordinates and the key's bit levels stay in registers.
+template <int D>
+__global__ void k_keys(const float* __restrict__ objs, uint64_t n, uint32_t is_rect, uint32_t mode,
+                       uint32_t bits, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const uint32_t stride = is_rect ? 2 * D : D;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
-    int64_t c[kMaxDims];
+    int64_t c[D];
     const float* o = objs + i * stride;
-    for (uint32_t d = 0; d < dims; ++d) {
-      float p = is_rect ? __fmul_rn(0.5f, __fadd_rn(o[d], o[dims + d])) : o[d];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      float p = is_rect ? __fmul_rn(0.5f, __fadd_rn(__ldg(o + d), __ldg(o + D + d))) : __ldg(o + d);
       c[d] = quantise(p, bits, mode);
     }
-    keys[i] = hilbert_index(dims, bits, c);
+    keys[i] = hilbert_index_t<D>(bits, c);
     vals[i] = (uint32_t)i;
   }
 }
@@ -468,26 +472,48 @@ template qcp_status exclusive_scan<uint64_t>(const uint64_t*, uint64_t*, uint64_
 qcp_status build_keys(const float* objs, uint64_t n, uint32_t dims, uint32_t is_rect,
                       uint32_t key_mode, uint32_t key_bits, uint64_t* keys, uint32_t* vals,
                       cudaStream_t s) {
-  k_keys<<<grid_for(n, 256, num_sms() * 16), 256, 0, s>>>(objs, n, dims, is_rect, key_mode, key_bits,
-                                                         keys, vals);
+  const uint32_t grid = grid_for(n, 256, num_sms() * 16);
+  QCP_DISPATCH_D(dims, (k_keys<DD><<<grid, 256, 0, s>>>(objs, n, is_rect, key_mode, key_bits, keys, vals)));
   note_launch();
   return check_launch("k_keys");
 }
 
+size_t radix_scratch_bytes(uint64_t n) {
+  const uint64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
+  const uint64_t hn = 256ull * ntiles;
+  return 2 * ((sizeof(uint32_t) * hn + 255) & ~(size_t)255) + scan_scratch_bytes(hn);
+}
+
 qcp_status radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp,
                             uint64_t n, uint32_t key_bits, DevPool& pool, cudaStream_t s,
-                            bool* result_in_tmp) {
+                            bool* result_in_tmp, void* scratch, size_t scratch_bytes) {
   *result_in_tmp = false;
   if (n <= 1) return QCP_OK;
   const uint32_t ntiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
   const uint64_t hn = 256ull * ntiles;
   void* hist = nullptr;
   void* offs = nullptr;
-  QCP_TRY(temp_alloc(sizeof(uint32_t) * hn, s, &hist));
-  qcp_status st = temp_alloc(sizeof(uint32_t) * hn, s, &offs);
-  if (st != QCP_OK) {
-    temp_free(hist, s);
-    return st;
+  void* sums = nullptr;  // the scan's chunk sums (caller scratch), else its own temporary
+  size_t sums_bytes = 0;
+  qcp_status st = QCP_OK;
+  if (scratch) {
+    // caller-owned scratch (a captured build): no allocation on the stream
+    if (scratch_bytes < radix_scratch_bytes(n)) {
+      set_error("radix_sort_pairs: scratch too small");
+      return QCP_ERR_BAD_ARG;
+    }
+    const size_t hb = (sizeof(uint32_t) * hn + 255) & ~(size_t)255;
+    hist = scratch;
+    offs = static_cast<char*>(scratch) + hb;
+    sums = static_cast<char*>(scratch) + 2 * hb;
+    sums_bytes = scan_scratch_bytes(hn);
+  } else {
+    QCP_TRY(temp_alloc(sizeof(uint32_t) * hn, s, &hist));
+    st = temp_alloc(sizeof(uint32_t) * hn, s, &offs);
+    if (st != QCP_OK) {
+      temp_free(hist, s);
+      return st;
+    }
   }
   uint64_t* kin = keys;
   uint32_t* vin = vals;
@@ -498,7 +524,7 @@ qcp_status radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, 
     const uint32_t shift = 8 * p;
     k_rs_upsweep<<<ntiles, RS_THREADS, 0, s>>>(kin, n, shift, (uint32_t*)hist, ntiles);
     note_launch();
-    st = exclusive_scan<uint32_t>((uint32_t*)hist, (uint32_t*)offs, hn, nullptr, pool, s);
+    st = exclusive_scan<uint32_t>((uint32_t*)hist, (uint32_t*)offs, hn, nullptr, pool, s, sums, sums_bytes);
     if (st != QCP_OK) break;
     k_rs_downsweep<<<ntiles, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n, shift, (uint32_t*)offs,
                                                  ntiles);
@@ -508,8 +534,10 @@ qcp_status radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, 
     std::swap(vin, vout);
     *result_in_tmp = !*result_in_tmp;
   }
-  temp_free(hist, s);
-  temp_free(offs, s);
+  if (!scratch) {
+    temp_free(hist, s);
+    temp_free(offs, s);
+  }
   return st;
 }
 

@@ -555,6 +555,7 @@ static qcp_status run_query(qcp_index* ix, const float* boxes, uint32_t q, const
   ws->timing = (o.flags & QCP_QUERY_TIMING) != 0;
   ws->blocks_per_sm = o.blocks_per_sm ? (o.blocks_per_sm > 32 ? 32u : o.blocks_per_sm) : 8u;
   ws->win_bits = o.win_bits ? (o.win_bits < 12 ? 12u : o.win_bits) : kDefaultWinBits;
+  ws->leaf_ring = leaf_ring_of(o.leaf_prefetch);
   ws->sort_small_jobs = ws->sort_msd_jobs = 0;
   ws->hybrid = o.algo == QCP_ALGO_HYBRID;
   ws->cpu_threads = o.cpu_threads;
@@ -647,11 +648,207 @@ static qcp_status run_query(qcp_index* ix, const float* boxes, uint32_t q, const
   return QCP_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Captured build (qcp_build_plan_*): the device bulk load of n objects of a
+// fixed shape -- keys, radix sort, packing, bottom-up MBR levels -- recorded
+// once into a CUDA graph over buffers the plan owns and replayed per build.
+// The reference builds on the host and copies the tree over in one piece
+// (Tree::Bottom_Up, src/tree/tree.cpp:410-495; MPHR::Build,
+// src/tree/mphr.cpp:60-133).
+// ---------------------------------------------------------------------------
+}  // namespace qcp
+
+struct qcp_build_plan {
+  qcp_index* ix = nullptr;
+  uint64_t n = 0;
+  uint32_t ncoord = 0;
+  float* d_in = nullptr;        // objects the graph reads (n rows of ncoord floats)
+  uint64_t* keys_tmp = nullptr;
+  uint32_t* vals = nullptr;
+  uint32_t* vals_tmp = nullptr;
+  uint32_t* bad = nullptr;      // nonzero: a coordinate was not finite
+  uint32_t* h_bad = nullptr;    // pinned mirror
+  void* rs_scratch = nullptr;
+  size_t rs_bytes = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace qcp {
+
+static void build_plan_destroy(qcp_build_plan* p) {
+  if (!p) return;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  cudaFree(p->d_in);
+  cudaFree(p->keys_tmp);
+  cudaFree(p->vals);
+  cudaFree(p->vals_tmp);
+  cudaFree(p->bad);
+  cudaFree(p->rs_scratch);
+  if (p->h_bad) cudaFreeHost(p->h_bad);
+  if (p->ix) index_release(p->ix);
+  delete p;
+}
+
+// The build's device work on stream s, allocation- and sync-free.
+static qcp_status build_plan_record(qcp_build_plan* p, cudaStream_t s) {
+  qcp_index* ix = p->ix;
+  QCP_CUDA(cudaMemsetAsync(p->bad, 0, sizeof(uint32_t), s));
+  QCP_TRY(build_keys(p->d_in, ix->n, ix->dims, ix->is_rect, ix->key_mode, ix->key_bits, ix->keys, p->vals, s));
+  bool in_tmp = false;
+  QCP_TRY(radix_sort_pairs(ix->keys, p->vals, p->keys_tmp, p->vals_tmp, ix->n, ix->dims * ix->key_bits, ix->pool, s,
+                           &in_tmp, p->rs_scratch, p->rs_bytes));
+  if (in_tmp)
+    QCP_CUDA(cudaMemcpyAsync(ix->keys, p->keys_tmp, sizeof(uint64_t) * ix->n, cudaMemcpyDeviceToDevice, s));
+  QCP_TRY(build_pack(ix, p->d_in, in_tmp ? p->vals_tmp : p->vals, s, p->bad));
+  QCP_TRY(build_levels(ix, s));
+  return QCP_OK;
+}
+
 }  // namespace qcp
 
 using namespace qcp;
 
 extern "C" {
+
+qcp_status qcp_build_plan_create(uint64_t n, uint32_t dims, uint32_t is_rect, const qcp_build_opts* opts,
+                                 qcp_build_plan** out) {
+  clear_error();
+  if (!out) {
+    set_error("out is NULL");
+    return QCP_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  qcp_build_opts o;
+  memset(&o, 0, sizeof(o));
+  if (opts) o = *opts;
+  if (n == 0 || n >= (1ull << 31) || dims < 1 || dims > (uint32_t)kMaxDims || is_rect > 1) {
+    set_error("qcp_build_plan_create: 1 <= n < 2^31, dims in [1, 8], is_rect 0 or 1");
+    return QCP_ERR_BAD_ARG;
+  }
+  const uint32_t fanout = o.fanout ? o.fanout : 128;
+  if (fanout < 32 || fanout > 256 || fanout % 32) {
+    set_error("fanout must be a multiple of 32 in [32, 256]");
+    return QCP_ERR_BAD_ARG;
+  }
+  if (o.key_mode > QCP_KEY_REF) {
+    set_error("qcp_build_plan_create: key_mode must be QCP_KEY_NORM or QCP_KEY_REF (the k-means keys iterate "
+              "to convergence on the host)");
+    return QCP_ERR_BAD_ARG;
+  }
+  const uint32_t bits = o.key_bits ? o.key_bits : default_bits(o.key_mode, dims);
+  if (bits > 32 || (uint64_t)bits * dims > 64) {
+    set_error("key bits per dimension must be <= 32 and dims*bits <= 64");
+    return QCP_ERR_BAD_ARG;
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    set_error("no CUDA device");
+    return QCP_ERR_NO_DEVICE;
+  }
+  qcp_build_plan* p = new (std::nothrow) qcp_build_plan();
+  if (!p) return QCP_ERR_OOM;
+  qcp_index* ix = new (std::nothrow) qcp_index();
+  if (!ix) {
+    delete p;
+    return QCP_ERR_OOM;
+  }
+  p->ix = ix;
+  cudaGetDevice(&ix->device);
+  ix->n = n;
+  ix->dims = dims;
+  ix->is_rect = is_rect;
+  ix->fanout = fanout;
+  ix->key_mode = o.key_mode;
+  ix->key_bits = bits;
+  ix->ncoord = is_rect ? 2 * dims : dims;
+  p->n = n;
+  p->ncoord = ix->ncoord;
+  p->rs_bytes = radix_scratch_bytes(n);
+  qcp_status st = index_alloc(ix);
+  cudaStream_t cap = nullptr;
+  if (st == QCP_OK) {
+    if (cudaMalloc(&p->d_in, sizeof(float) * p->ncoord * n) != cudaSuccess ||
+        cudaMalloc(&p->keys_tmp, sizeof(uint64_t) * n) != cudaSuccess ||
+        cudaMalloc(&p->vals, sizeof(uint32_t) * n) != cudaSuccess ||
+        cudaMalloc(&p->vals_tmp, sizeof(uint32_t) * n) != cudaSuccess ||
+        cudaMalloc(&p->bad, sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&p->rs_scratch, p->rs_bytes) != cudaSuccess ||
+        cudaMallocHost(&p->h_bad, sizeof(uint32_t)) != cudaSuccess) {
+      st = cuda_status(cudaGetLastError(), "qcp_build_plan_create allocation");
+      if (st == QCP_OK) st = QCP_ERR_OOM;
+    }
+  }
+  if (st == QCP_OK && cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess)
+    st = cuda_status(cudaGetLastError(), "cudaStreamCreate");
+  if (st == QCP_OK) {
+    // the build's attributes and lazily loaded kernels are set up by one
+    // uncaptured run over the (zeroed) input before the capture
+    cudaMemsetAsync(p->d_in, 0, sizeof(float) * p->ncoord * n, cap);
+    st = build_plan_record(p, cap);
+    if (st == QCP_OK && cudaStreamSynchronize(cap) != cudaSuccess) st = cuda_status(cudaGetLastError(), "build");
+  }
+  if (st == QCP_OK) {
+    if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      st = cuda_status(cudaGetLastError(), "cudaStreamBeginCapture");
+    } else {
+      st = build_plan_record(p, cap);
+      cudaGraph_t g = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(cap, &g);
+      if (st == QCP_OK && e != cudaSuccess) st = cuda_status(e, "cudaStreamEndCapture");
+      p->graph = g;
+      if (st == QCP_OK && cudaGraphInstantiate(&p->exec, p->graph, 0) != cudaSuccess)
+        st = cuda_status(cudaGetLastError(), "cudaGraphInstantiate");
+    }
+  }
+  if (cap) cudaStreamDestroy(cap);
+  if (st != QCP_OK) {
+    build_plan_destroy(p);
+    return st;
+  }
+  *out = p;
+  return QCP_OK;
+}
+
+float* qcp_build_plan_input(qcp_build_plan* p) { return p ? p->d_in : nullptr; }
+
+qcp_status qcp_build_plan_run(qcp_build_plan* p, const float* objs, uint32_t objs_mem, void* stream,
+                              qcp_index** index) {
+  clear_error();
+  if (!p || !index || objs_mem > QCP_MEM_DEVICE) {
+    set_error("qcp_build_plan_run: plan and index must be non-NULL, objs_mem a qcp_mem");
+    return QCP_ERR_BAD_ARG;
+  }
+  *index = nullptr;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (objs && objs != p->d_in)
+    QCP_CUDA(cudaMemcpyAsync(p->d_in, objs, sizeof(float) * p->ncoord * p->n,
+                             objs_mem == QCP_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  QCP_CUDA(cudaGraphLaunch(p->exec, s));
+  note_launch();
+  QCP_CUDA(cudaMemcpyAsync(p->h_bad, p->bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  QCP_CUDA(cudaStreamSynchronize(s));
+  {
+    std::lock_guard<std::mutex> g(p->ix->host_mbr_mu);
+    p->ix->host_mbr_ready = false;  // host copies of the old levels are stale
+  }
+  if (*p->h_bad) {
+    set_error("object coordinates must be finite");
+    return QCP_ERR_BAD_ARG;
+  }
+  *index = p->ix;
+  return QCP_OK;
+}
+
+qcp_status qcp_build_plan_free(qcp_build_plan* p) {
+  clear_error();
+  if (!p) return QCP_OK;
+  cudaDeviceSynchronize();
+  build_plan_destroy(p);
+  return QCP_OK;
+}
 
 const char* qcp_last_error(void) { return t_error.c_str(); }
 

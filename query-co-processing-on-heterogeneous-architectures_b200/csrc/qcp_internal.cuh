@@ -115,6 +115,7 @@ struct Workspace {
   uint32_t hist_G = 0, hist_bits = 0;
   uint32_t blocks_per_sm = 8;    // traversal grid = SMs x this, this call
   uint32_t win_bits = 18;        // sort window, this call
+  uint32_t leaf_ring = 2;        // leaf prefetch buffers per warp, this call (< 2: none)
   // CPU + GPU co-processing (QCP_ALGO_HYBRID) of this call
   bool hybrid = false;
   uint32_t cpu_threads = 0, handoff_level = 1;
@@ -151,6 +152,7 @@ enum CtrSlot : uint32_t {
   kCtrJobs1 = 6,
   kCtrSmall = 7,      // small-segment job count
   kCtrWork2 = 8,
+  kCtrTimeout = 9,    // nonzero: a bounded device wait ran out (results invalid)
   kCtrCount = 16
 };
 
@@ -204,29 +206,70 @@ __host__ __device__ __forceinline__ uint64_t low_ones64(uint32_t k) {
   return k >= 64 ? ~0ull : ((1ull << k) - 1ull);
 }
 
+__host__ __device__ __forceinline__ uint32_t clz64(uint64_t x) {
+#ifdef __CUDA_ARCH__
+  return (uint32_t)__clzll((long long)x);
+#else
+  return x ? (uint32_t)__builtin_clzll(x) : 64u;
+#endif
+}
+
+// Bit b of x moved to bit D*b (b < 64/D): "dilation" by the binary magic
+// numbers method (shift-or-mask rounds, as in S. E. Anderson's Bit
+// Twiddling Hacks, "Interleave bits by Binary Magic Numbers"; R. Raman and
+// D. S. Wise, "Converting to and from Dilated Integers", IEEE TC 2008) for
+// D = 2 and 3, a plain loop otherwise.
+template <int D>
+__host__ __device__ __forceinline__ uint64_t dilate(uint64_t x, uint32_t bits) {
+  if (D == 2) {
+    x &= 0xffffffffull;
+    x = (x | (x << 16)) & 0x0000ffff0000ffffull;
+    x = (x | (x << 8)) & 0x00ff00ff00ff00ffull;
+    x = (x | (x << 4)) & 0x0f0f0f0f0f0f0f0full;
+    x = (x | (x << 2)) & 0x3333333333333333ull;
+    x = (x | (x << 1)) & 0x5555555555555555ull;
+    return x;
+  } else if (D == 3) {
+    x &= 0x1fffffull;
+    x = (x | (x << 32)) & 0x001f00000000ffffull;
+    x = (x | (x << 16)) & 0x001f0000ff0000ffull;
+    x = (x | (x << 8)) & 0x100f00f00f00f00full;
+    x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+  } else {
+    uint64_t t = 0;
+    for (uint32_t b = 0; b < bits; ++b) t |= ((x >> b) & 1ull) << (b * D);
+    return t;
+  }
+}
+
 // Hilbert index of integer coordinates, the algorithm of
 // HilbertMapper::MappingIntoSingle (src/mapper/hilbert_mapper.cpp:25-64) and
-// hilbert_macro.h:4-22, written in unsigned 64-bit arithmetic.
-__host__ __device__ inline uint64_t hilbert_index(uint32_t dims, uint32_t bits, const int64_t* coord) {
-  if (dims <= 1) return (uint64_t)coord[0];
+// hilbert_macro.h:4-22, written in unsigned 64-bit arithmetic: the
+// coordinates are packed (coordinate d at bits [d*bits, (d+1)*bits), wider
+// values spilling into the next field as in the reference's shifts), the
+// fields are transposed into bit levels (level b holds bit b of every
+// coordinate, coordinate d at bit d), then Gray-coded level by level with the
+// entry-point rotation, and prefix-XORed.
+template <int D>
+__host__ __device__ inline uint64_t hilbert_index_t(uint32_t bits, const int64_t* coord) {
+  if (D <= 1) return (uint64_t)coord[0];
+  constexpr uint32_t dims = (uint32_t)D;
   const uint32_t total = dims * bits;
   uint64_t packed = 0;
-  for (int d = (int)dims - 1; d >= 0; --d) {
+  for (int d = D - 1; d >= 0; --d) {
     packed = (packed << bits) | (uint64_t)coord[d];
   }
   // transpose: level b holds bit b of every coordinate (coordinate d at bit d)
   uint64_t t = 0;
-  for (uint32_t b = 0; b < bits; ++b) {
-    for (uint32_t d = 0; d < dims; ++d) {
-      t |= ((packed >> (d * bits + b)) & 1ull) << (b * dims + d);
-    }
-  }
+  const uint64_t field = low_ones64(bits);
+  for (uint32_t d = 0; d < dims; ++d) t |= dilate<D>((packed >> (d * bits)) & field, bits) << d;
   uint64_t index;
   if (bits > 1) {
-    const uint64_t nd_ones = low_ones64(dims);
-    const uint64_t nd1_ones = nd_ones >> 1;
-    uint64_t level_low = 0;
-    for (uint32_t b = 0; b < bits; ++b) level_low |= 1ull << (b * dims);
+    constexpr uint64_t nd_ones = (1ull << dims) - 1ull;
+    constexpr uint64_t nd1_ones = nd_ones >> 1;
+    const uint64_t level_low = dilate<D>(field, bits);  // bit 0 of every level
     t ^= t >> dims;
     index = 0;
     uint32_t rot = 0;
@@ -236,11 +279,9 @@ __host__ __device__ inline uint64_t hilbert_index(uint32_t dims, uint32_t bits, 
       if (rot) g = ((g >> rot) | (g << (dims - rot))) & nd_ones;
       index = (index << dims) | g;
       flip = 1ull << rot;
-      uint64_t low = g & (0ull - g) & nd1_ones;
-      while (low) {
-        low >>= 1;
-        ++rot;
-      }
+      // the rotation advances past the lowest set bit of g below the top one
+      const uint64_t low = g & (0ull - g) & nd1_ones;
+      if (low) rot += 64u - clz64(low);
       if (++rot >= dims) rot -= dims;
     }
     index ^= level_low >> 1;
@@ -249,6 +290,19 @@ __host__ __device__ inline uint64_t hilbert_index(uint32_t dims, uint32_t bits, 
   }
   for (uint32_t s = 1; s < total; s *= 2) index ^= index >> s;
   return index & low_ones64(total);
+}
+
+__host__ __device__ inline uint64_t hilbert_index(uint32_t dims, uint32_t bits, const int64_t* coord) {
+  switch (dims) {
+    case 1: return hilbert_index_t<1>(bits, coord);
+    case 2: return hilbert_index_t<2>(bits, coord);
+    case 3: return hilbert_index_t<3>(bits, coord);
+    case 4: return hilbert_index_t<4>(bits, coord);
+    case 5: return hilbert_index_t<5>(bits, coord);
+    case 6: return hilbert_index_t<6>(bits, coord);
+    case 7: return hilbert_index_t<7>(bits, coord);
+    default: return hilbert_index_t<8>(bits, coord);
+  }
 }
 
 // One per-query slice handed to the sort kernels: output offset, size and
@@ -271,9 +325,12 @@ int num_sms();
 qcp_status build_keys(const float* objs, uint64_t n, uint32_t dims, uint32_t is_rect,
                       uint32_t key_mode, uint32_t key_bits, uint64_t* keys, uint32_t* vals,
                       cudaStream_t s);
+// With `scratch` (at least radix_scratch_bytes(n)) nothing is allocated, so
+// the sort can be captured into a graph.
 qcp_status radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp,
                             uint64_t n, uint32_t key_bits, DevPool& pool, cudaStream_t s,
-                            bool* result_in_tmp);
+                            bool* result_in_tmp, void* scratch = nullptr, size_t scratch_bytes = 0);
+size_t radix_scratch_bytes(uint64_t n);
 qcp_status build_keys_kmeans(const float* objs, uint64_t n, uint32_t dims, uint32_t is_rect, uint32_t bits,
                              uint32_t K, uint32_t max_iters, uint64_t* keys, uint32_t* vals, cudaStream_t s);
 uint32_t kmeans_rank_bits(uint32_t K);
@@ -303,6 +360,15 @@ qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void*
 size_t sort_tables_bytes(const qcp_index* ix, const Workspace* ws, uint32_t q);
 // Window bits and window count of the per-query sort for this call.
 void sort_window_shape(const qcp_index* ix, const Workspace* ws, uint32_t* wbits, uint32_t* G);
+// Leaf prefetch buffers per warp of the traversal's leaf passes for a
+// qcp_query_opts.leaf_prefetch value: 0 = the default (2), 1 = none (direct
+// loads), 2..4 = that many.
+constexpr uint32_t kDefaultLeafRing = 2;
+inline uint32_t leaf_ring_of(uint32_t knob) {
+  if (knob == 0) return kDefaultLeafRing;
+  if (knob == 1) return 0;
+  return knob > 4 ? 4u : knob;
+}
 // Largest window count whose per-window counts the write pass gathers.
 constexpr uint32_t kHistMaxG = 256;
 // Default log2 of the per-query sort's id windows (qcp_query_opts.win_bits).

@@ -65,13 +65,17 @@ qcp_status scratch_on_current_device(NoAllocScratch** out) {
   return QCP_OK;
 }
 
-bool is_device_pointer(const void* p) {
+// Memory the kernels on `device` may read and write: device memory of that
+// GPU, or managed memory.  Device memory of another GPU is refused: without
+// peer access a kernel that touched it would fault.
+bool is_device_pointer_on(const void* p, int device) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == device;
 }
 
 }  // namespace
@@ -92,14 +96,14 @@ extern "C" qcp_status qcp_query_counts_noalloc(qcp_index* index, const float* d_
     set_error("qcp_query_counts_noalloc takes at most 262144 queries per call");
     return QCP_ERR_BAD_ARG;
   }
-  if (!d_boxes || !d_counts || !is_device_pointer(d_boxes) || !is_device_pointer(d_counts)) {
-    set_error("qcp_query_counts_noalloc needs device-memory boxes and counts");
-    return QCP_ERR_BAD_ARG;
-  }
   int dev = 0;
-  cudaGetDevice(&dev);
+  QCP_CUDA(cudaGetDevice(&dev));
   if (dev != index->device) {
     set_error("index lives on another device than the current one");
+    return QCP_ERR_BAD_ARG;
+  }
+  if (!d_boxes || !d_counts || !is_device_pointer_on(d_boxes, dev) || !is_device_pointer_on(d_counts, dev)) {
+    set_error("qcp_query_counts_noalloc needs boxes and counts in device memory of the index's device");
     return QCP_ERR_BAD_ARG;
   }
   NoAllocScratch* sc = nullptr;

@@ -79,6 +79,7 @@ extern "C" qcp_status qcp_plan_create(qcp_index* ix, uint32_t max_queries, uint6
   Workspace* ws = p->ws;
   ws->blocks_per_sm = (opts && opts->blocks_per_sm) ? (opts->blocks_per_sm > 32 ? 32u : opts->blocks_per_sm) : 8u;
   ws->win_bits = (opts && opts->win_bits) ? (opts->win_bits < 12 ? 12u : opts->win_bits) : kDefaultWinBits;
+  ws->leaf_ring = leaf_ring_of(opts ? opts->leaf_prefetch : 0u);
   qcp_status st = QCP_OK;
   do {
     const size_t row = 2 * (size_t)ix->dims;
@@ -204,6 +205,10 @@ extern "C" qcp_status qcp_plan_run(qcp_plan* p, const float* boxes, uint32_t q, 
   QCP_CUDA(cudaMemcpyAsync(ws->h_ctr, ws->ctr, sizeof(uint32_t) * kCtrCount, cudaMemcpyDeviceToHost, s));
   QCP_CUDA(cudaMemcpyAsync(ws->h_total, ws->offsets + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   QCP_CUDA(cudaStreamSynchronize(s));
+  if (ws->h_ctr[kCtrTimeout]) {
+    set_error("qcp_plan_run: a bounded wait for a leaf's bulk copy ran out");
+    return QCP_ERR_TIMEOUT;
+  }
   const uint32_t flags = ws->h_ctr[kCtrOverflow];
   if (flags & 1u) {
     set_error("qcp_plan_run: the batch's traversal frontier exceeded the plan's item capacity");

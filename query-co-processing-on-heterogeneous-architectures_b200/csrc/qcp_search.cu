@@ -84,9 +84,28 @@ __global__ void __launch_bounds__(256) k_expand(const float* __restrict__ boxes,
 
 enum { kCount = 0, kWrite = 1 };
 
+// Shared memory of one warp's leaf prefetch ring: kRingHeader bytes of
+// mbarriers (one per buffer) and the list of the current item's partially
+// covered leaves (offsets in the item), then `nbuf` leaf buffers of NR runs
+// of F floats (the leaf's coordinate runs; in the write pass its ids too).
+constexpr uint32_t kRingHeader = 384;
+constexpr uint32_t kRingMaxBuf = 4;
+
+__host__ __device__ constexpr uint32_t leaf_runs(int D, bool rect, int mode) {
+  return (rect ? 2u * D : (uint32_t)D) + (mode == kWrite ? 1u : 0u);
+}
+__host__ __device__ inline uint32_t ring_warp_bytes(uint32_t runs, uint32_t F, uint32_t nbuf) {
+  return kRingHeader + nbuf * runs * F * 4u;
+}
+
 // Warp per (query, level-1 node) item.  COUNT: item_hits[i] and qcount[q].
 // WRITE: ids at out[offsets[q] + reserved slice].
-template <int D, bool RECT, int MODE>
+// PF: the partially covered leaves of an item are fetched into the warp's
+// shared-memory ring by bulk copies (cp.async.bulk on the TMA unit, nbuf
+// leaves ahead, completion on one mbarrier per buffer) while the warp tests
+// the leaf before; without PF every lane loads its float4s from global
+// memory.  A bulk-copy wait that runs out sets err[0] and the warp stops.
+template <int D, bool RECT, int MODE, bool PF>
 __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __restrict__ boxes,
                                                   const uint2* __restrict__ items,
                                                   const uint32_t* __restrict__ item_count,
@@ -96,19 +115,38 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
                                                   unsigned long long* qcursor,
                                                   int32_t* __restrict__ out, uint64_t item_cap,
                                                   unsigned long long* stats, uint32_t* qwhist, uint32_t hist_G,
-                                                  uint32_t hist_bits) {
+                                                  uint32_t hist_bits, uint32_t nbuf, uint32_t* err) {
   // write pass of the sorted path: per-(query, window) id counts in per-warp
   // shared counters, flushed once per item
   __shared__ uint32_t wcount[8][MODE == kWrite ? kHistMaxG : 1];
+  extern __shared__ __align__(128) unsigned char ring_raw[];
+  constexpr uint32_t NC = RECT ? 2 * D : D;       // coordinate runs of a leaf
+  constexpr uint32_t NR = leaf_runs(D, RECT, MODE);
   const uint32_t lane = threadIdx.x & 31;
-  uint32_t* wc = wcount[(threadIdx.x >> 5) & 7];
+  const uint32_t wib = (threadIdx.x >> 5) & 7;
+  uint32_t* wc = wcount[wib];
   const bool hist = MODE == kWrite && qwhist != nullptr;
   if (hist) {
     for (uint32_t w = lane; w < hist_G; w += 32) wc[w] = 0;
     __syncwarp();
   }
-  const uint32_t nitems = (uint32_t)min((uint64_t)*item_count, item_cap);
   const uint32_t F = t.fanout;
+  unsigned char* ring = ring_raw + (size_t)wib * (PF ? ring_warp_bytes(NR, F, nbuf) : 0u);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring);
+  uint8_t* plist = ring + 64;
+  float* bufs = reinterpret_cast<float*>(ring + kRingHeader);
+  const uint32_t buf_floats = NR * F;
+  uint32_t phase = 0;     // bit b: parity of buffer b's next completion
+  uint32_t pending = 0;   // bit b: a copy into buffer b has not been waited for
+  bool dead = false;      // a bulk-copy wait ran out
+  if (PF) {
+    if (lane == 0) {
+      for (uint32_t b = 0; b < nbuf; ++b) mbar_init(&bars[b], 1);
+      mbar_fence_init();
+    }
+    __syncwarp();
+  }
+  const uint32_t nitems = (uint32_t)min((uint64_t)*item_count, item_cap);
   const float* lmbr = t.mbr[0];
   const uint64_t lpad = t.pad[0];
   const uint64_t nleaves = t.nodes[0];
@@ -128,6 +166,7 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
     }
     uint32_t hits = 0;  // per lane (count mode)
     uint32_t n_cov = 0, n_part = 0, o_cov = 0;  // per lane work counters (count mode)
+    uint32_t npart = 0;  // PF: partially covered leaves listed for the ring
     const uint64_t l0 = (uint64_t)it.y * F;
     const uint64_t l1 = (l0 + F < nleaves) ? l0 + F : nleaves;
     for (uint64_t lb = l0; lb < l1; lb += 32) {
@@ -185,8 +224,14 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
           wpos += cnt;
         }
       }
-      // partially covered leaves: test every object
       uint32_t mp = mov & ~min_;
+      if constexpr (PF) {
+        // listed for the prefetch ring below
+        if ((mp >> lane) & 1u) plist[npart + __popc(mp & lane_lt_mask())] = (uint8_t)(lb - l0 + lane);
+        npart += __popc(mp);
+        mp = 0;
+      }
+      // partially covered leaves: test every object
       while (mp) {
         const int s = __ffs(mp) - 1;
         mp &= mp - 1;
@@ -219,6 +264,68 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
         }
       }
     }
+    if (PF && npart) {
+      // partially covered leaves through the ring: leaf k of the list goes
+      // to buffer k % nbuf, nbuf leaves ahead of the one being tested
+      __syncwarp();  // the list is complete
+      const uint32_t run_bytes = F * 4u;
+      auto issue = [&](uint32_t k, uint32_t bb) {
+        const uint64_t leaf = l0 + plist[k];
+        fence_proxy_async_smem();  // this buffer's earlier reads before the copy
+        __syncwarp();
+        if (lane == 0) mbar_arrive_expect_tx(&bars[bb], NR * run_bytes);
+        __syncwarp();
+        if (lane < NR) {
+          const void* src = (lane < NC) ? (const void*)(t.coords + (uint64_t)lane * t.npad + leaf * F)
+                                        : (const void*)(t.ids + leaf * F);
+          bulk_copy_g2s(bufs + (size_t)bb * buf_floats + lane * F, src, run_bytes, &bars[bb]);
+        }
+        pending |= 1u << bb;
+      };
+      const uint32_t pre = npart < nbuf ? npart : nbuf;
+      for (uint32_t k = 0; k < pre; ++k) issue(k, k);
+      uint32_t bb = 0;
+      for (uint32_t k = 0; k < npart; ++k) {
+        const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(&bars[bb], (phase >> bb) & 1u));
+        if (!ok) {
+          dead = true;
+          break;
+        }
+        phase ^= 1u << bb;
+        pending &= ~(1u << bb);
+        const float* sb = bufs + (size_t)bb * buf_floats;
+        const uint64_t e0 = (l0 + plist[k]) * F;
+        const uint32_t valid = (t.n > e0) ? (uint32_t)min((uint64_t)F, t.n - e0) : 0u;
+        for (uint32_t g0 = 0; g0 < F; g0 += 128) {  // warp-uniform trip count
+          const uint32_t g = g0 + lane * 4;
+          const uint32_t hm = (g < F) ? test4_staged<D, RECT>(b, sb, F, g, valid) : 0u;
+          if (MODE == kCount) {
+            hits += __popc(hm);
+          } else {
+            uint32_t tot;
+            const uint32_t ex = warp_excl_sum(__popc(hm), &tot);
+            if (hm) {
+              const int4 idv = *reinterpret_cast<const int4*>(sb + NC * F + g);
+              uint64_t o = wpos + ex;
+              if (hm & 1u) out[o++] = idv.x;
+              if (hm & 2u) out[o++] = idv.y;
+              if (hm & 4u) out[o++] = idv.z;
+              if (hm & 8u) out[o++] = idv.w;
+              if (hist) {
+                if (hm & 1u) atomicAdd(wc + ((uint32_t)idv.x >> hist_bits), 1u);
+                if (hm & 2u) atomicAdd(wc + ((uint32_t)idv.y >> hist_bits), 1u);
+                if (hm & 4u) atomicAdd(wc + ((uint32_t)idv.z >> hist_bits), 1u);
+                if (hm & 8u) atomicAdd(wc + ((uint32_t)idv.w >> hist_bits), 1u);
+              }
+            }
+            wpos += tot;
+          }
+        }
+        if (k + nbuf < npart) issue(k + nbuf, bb);
+        bb = (bb + 1 == nbuf) ? 0u : bb + 1;
+      }
+      if (dead) break;
+    }
     if (hist) {
       __syncwarp();
       for (uint32_t w = lane; w < hist_G; w += 32) {
@@ -246,6 +353,13 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
         if (o_cov) atomicAdd(stats + kStatObjCovered, (unsigned long long)o_cov);
       }
     }
+  }
+  if (PF && dead) {
+    if (lane == 0) atomicOr(err, 1u);
+    // copies still in flight land in this warp's ring: wait for them (again
+    // bounded) before the CTA's shared memory goes away
+    for (uint32_t bb = 0; bb < nbuf; ++bb)
+      if ((pending >> bb) & 1u) mbar_wait_bounded(&bars[bb], (phase >> bb) & 1u);
   }
 }
 
@@ -391,23 +505,57 @@ void launch_expand(uint32_t grid, cudaStream_t s, const float* boxes, const uint
                                    child_pad, fanout, overflow, need);
 }
 
+// Ring buffers per warp that fit the leaf prefetch of this launch: at most
+// `want` (kRingMaxBuf), fewer when eight warps' rings would not leave room
+// for two CTAs per SM; 0 = no ring (direct loads).
+inline uint32_t ring_buffers(uint32_t runs, uint32_t F, uint32_t want) {
+  if (want < 2) return 0;
+  uint32_t nb = want > kRingMaxBuf ? kRingMaxBuf : want;
+  while (nb >= 2 && 8u * ring_warp_bytes(runs, F, nb) > 100u * 1024u) --nb;
+  return nb >= 2 ? nb : 0;
+}
+
+template <int D, bool RECT, int MODE>
+void launch_leafscan_t(uint32_t grid, cudaStream_t s, const TreeView& t, const float* boxes, const uint2* items,
+                       const uint32_t* item_count, uint32_t* work, uint32_t* item_hits, uint64_t* qcount,
+                       const uint64_t* offsets, uint64_t* qcursor, int32_t* out, uint64_t item_cap,
+                       unsigned long long* stats, uint32_t* qwhist, uint32_t hist_G, uint32_t hist_bits,
+                       uint32_t ring, uint32_t* err) {
+  const uint32_t nb = ring_buffers(leaf_runs(D, RECT, MODE), t.fanout, ring);
+  if (nb) {
+    const size_t smem = 8u * (size_t)ring_warp_bytes(leaf_runs(D, RECT, MODE), t.fanout, nb);
+    auto* kern = k_leafscan<D, RECT, MODE, true>;
+    if (smem > 48u * 1024u) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // no more CTAs than fit on the SMs at once (the static counters and 1 KB
+    // per CTA of reserved shared memory included)
+    const size_t per_cta = smem + sizeof(uint32_t) * 8 * (MODE == kWrite ? kHistMaxG : 1) + 1024;
+    const uint32_t fit = (uint32_t)((228u * 1024u) / per_cta);
+    const uint32_t sms = (uint32_t)num_sms();
+    if (fit >= 1 && grid > sms * fit) grid = sms * fit;
+    kern<<<grid, 256, smem, s>>>(t, boxes, items, item_count, work, item_hits, (unsigned long long*)qcount,
+                                 (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap,
+                                 stats, qwhist, hist_G, hist_bits, nb, err);
+  } else {
+    k_leafscan<D, RECT, MODE, false><<<grid, 256, 0, s>>>(
+        t, boxes, items, item_count, work, item_hits, (unsigned long long*)qcount,
+        (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap, stats, qwhist, hist_G,
+        hist_bits, 0u, err);
+  }
+}
+
 template <int D, int MODE>
 void launch_leafscan(bool rect, uint32_t grid, cudaStream_t s, const TreeView& t, const float* boxes,
                      const uint2* items, const uint32_t* item_count, uint32_t* work,
                      uint32_t* item_hits, uint64_t* qcount, const uint64_t* offsets,
                      uint64_t* qcursor, int32_t* out, uint64_t item_cap,
-                     unsigned long long* stats, uint32_t* qwhist = nullptr, uint32_t hist_G = 0,
-                     uint32_t hist_bits = 0) {
+                     unsigned long long* stats, uint32_t* qwhist, uint32_t hist_G,
+                     uint32_t hist_bits, uint32_t ring, uint32_t* err) {
   if (rect)
-    k_leafscan<D, true, MODE><<<grid, 256, 0, s>>>(
-        t, boxes, items, item_count, work, item_hits, (unsigned long long*)qcount,
-        (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap, stats, qwhist, hist_G,
-        hist_bits);
+    launch_leafscan_t<D, true, MODE>(grid, s, t, boxes, items, item_count, work, item_hits, qcount, offsets, qcursor,
+                                     out, item_cap, stats, qwhist, hist_G, hist_bits, ring, err);
   else
-    k_leafscan<D, false, MODE><<<grid, 256, 0, s>>>(
-        t, boxes, items, item_count, work, item_hits, (unsigned long long*)qcount,
-        (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap, stats, qwhist, hist_G,
-        hist_bits);
+    launch_leafscan_t<D, false, MODE>(grid, s, t, boxes, items, item_count, work, item_hits, qcount, offsets,
+                                      qcursor, out, item_cap, stats, qwhist, hist_G, hist_bits, ring, err);
 }
 
 template <int D, int MODE>
@@ -458,7 +606,7 @@ qcp_status write_items(qcp_index* ix, Workspace* ws, int cur, cudaStream_t s) {
                                                        ws->item_hits, nullptr, ws->offsets, ws->qcursor,
                                                        ws->out_ids, ws->items_cap, ws->d_stats,
                                                        ws->hist_G ? ws->qwhist : nullptr, ws->hist_G,
-                                                       ws->hist_bits));
+                                                       ws->hist_bits, ws->leaf_ring, ctr + kCtrTimeout));
   note_launch();
   return check_launch("k_leafscan<write>");
 }
@@ -506,7 +654,8 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
     QCP_DISPATCH_D(D, launch_leafscan<DD, kCount>(rect, grid, s, t, ws->boxes, ws->items[cur],
                                                   ctr + kCtrFrontier0 + cur, ctr + kCtrWork,
                                                   ws->item_hits, ws->qcount, nullptr, nullptr, nullptr,
-                                                  ws->items_cap, ws->d_stats));
+                                                  ws->items_cap, ws->d_stats, nullptr, 0, 0, ws->leaf_ring,
+                                                  ctr + kCtrTimeout));
     note_launch();
     QCP_TRY(check_launch("k_leafscan<count>"));
     mark(ws, kEvCount, s);
@@ -516,6 +665,10 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
     QCP_CUDA(cudaMemcpyAsync(ws->h_ctr, ctr, sizeof(uint32_t) * kCtrCount, cudaMemcpyDeviceToHost, s));
     QCP_CUDA(cudaMemcpyAsync(ws->h_total, ws->offsets + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
     QCP_CUDA(cudaStreamSynchronize(s));
+    if (ws->h_ctr[kCtrTimeout]) {
+      set_error("a bounded wait for a leaf's bulk copy ran out in the count pass");
+      return QCP_ERR_TIMEOUT;
+    }
     if (ws->h_ctr[kCtrOverflow]) {
       size_t need = (size_t)ws->h_ctr[kCtrNeedItems];
       if (need < ws->items_cap * 2) need = ws->items_cap * 2;
@@ -543,6 +696,15 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
       mark(ws, kEvWrite, s);
       if (sort) QCP_TRY(segmented_sort(ix, ws, q, s));
       mark(ws, kEvSort, s);
+      if (ws->leaf_ring >= 2) {
+        QCP_CUDA(cudaMemcpyAsync(ws->h_ctr + kCtrTimeout, ctr + kCtrTimeout, sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, s));
+        QCP_CUDA(cudaStreamSynchronize(s));
+        if (ws->h_ctr[kCtrTimeout]) {
+          set_error("a bounded wait for a leaf's bulk copy ran out in the write pass");
+          return QCP_ERR_TIMEOUT;
+        }
+      }
     }
     return QCP_OK;
   }
@@ -616,7 +778,7 @@ qcp_status run_batched_counts_into(qcp_index* ix, const float* boxes, uint32_t q
   }
   QCP_DISPATCH_D(D, launch_leafscan<DD, kCount>(rect, grid, s, t, boxes, items[cur], ctr + kCtrFrontier0 + cur,
                                                 ctr + kCtrWork, item_hits, counts, nullptr, nullptr, nullptr,
-                                                item_cap, stats));
+                                                item_cap, stats, nullptr, 0, 0, 0, ctr + kCtrTimeout));
   note_launch();
   QCP_TRY(check_launch("batched counts"));
   uint32_t overflow = 0;  // pageable host word: no pinned buffer is allocated
@@ -656,7 +818,7 @@ qcp_status run_batched_device(qcp_index* ix, Workspace* ws, uint32_t q, uint64_t
   QCP_DISPATCH_D(D, launch_leafscan<DD, kCount>(rect, grid, s, t, ws->boxes, ws->items[cur],
                                                 ctr + kCtrFrontier0 + cur, ctr + kCtrWork, ws->item_hits,
                                                 ws->qcount, nullptr, nullptr, nullptr, ws->items_cap,
-                                                ws->d_stats));
+                                                ws->d_stats, nullptr, 0, 0, ws->leaf_ring, ctr + kCtrTimeout));
   note_launch();
   QCP_TRY(exclusive_scan_counts(ws->qcount, ws->offsets, q, ix->pool, s, ws->scan_tmp, ws->scan_tmp_cap));
   k_gate<<<1, 32, 0, s>>>((const unsigned long long*)ws->offsets, q, ids_cap, ctr + kCtrFrontier0 + cur,

@@ -6,6 +6,8 @@
 // The ids of one slice are distinct and lie in [0, n), so only the low
 // `idbits` = ceil(log2 n) bits carry order.
 //
+//   slice <= kTinyCap ids   one warp bucket-sorts it in shared memory (256
+//                           buckets, a few ids each, insertion-sorted);
 //   slice <= kSmallCap ids  one CTA bucket-sorts it in shared memory: ids
 //                           are counted into 2048 buckets by their top bits
 //                           (the atomic's return value is the id's slot in
@@ -32,6 +34,10 @@ namespace qcp {
 
 namespace {
 
+// ---- tiny slices (one warp each) --------------------------------------------
+constexpr uint32_t kTinyCap = 1024;                    // ids of a slice sorted by one warp
+constexpr uint32_t kTinyBuckets = 256;                 // buckets of the warp's counting pass
+constexpr uint32_t kTinyWarps = 8;                     // warps per CTA
 // ---- small slices ----------------------------------------------------------
 constexpr uint32_t kSmallCap = kSmallSliceCap;
 constexpr uint32_t kSmallThreads = 256;
@@ -74,6 +80,86 @@ struct BucketSmem {
   uint32_t wtot[kSmallWarps];
 };
 
+// Slices of at most kTinyCap ids, one warp each (no CTA barriers): the ids
+// are counted into kTinyBuckets buckets by their top bits, a warp scan gives
+// the bucket bases, every id (read again, from L2) takes the next slot of its
+// bucket, each lane insertion-sorts its 8 buckets (a few ids each) and the
+// slice leaves in coalesced stores.  Jobs of more ids are k_sort_small's.
+struct TinySmem {
+  uint32_t stage[kTinyWarps][kTinyCap];
+  uint32_t cnt[kTinyWarps][kTinyBuckets];
+  uint32_t base[kTinyWarps][kTinyBuckets];
+};
+
+__global__ void __launch_bounds__(kTinyWarps * 32) k_sort_tiny(const Job* __restrict__ jobs,
+                                                               const uint32_t* __restrict__ njobs_p,
+                                                               int32_t* out, uint32_t idbits) {
+  const uint32_t njobs = *njobs_p;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TinySmem& sm = *reinterpret_cast<TinySmem*>(smem_raw);
+  const uint32_t lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  uint32_t* stage = sm.stage[wp];
+  uint32_t* cnt = sm.cnt[wp];
+  uint32_t* base = sm.base[wp];
+  constexpr uint32_t kPer = kTinyBuckets / 32;  // buckets per lane
+  const uint32_t bshift = idbits > 8 ? idbits - 8 : 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kPer; ++k) cnt[lane * kPer + k] = 0;
+  __syncwarp();
+  const uint32_t warps = gridDim.x * kTinyWarps;
+  for (uint32_t j = blockIdx.x * kTinyWarps + wp; j < njobs; j += warps) {
+    const Job jb = jobs[j];
+    const uint32_t size = jb.size;
+    if (size > kTinyCap) continue;  // warp-uniform
+    const int32_t* src = out + jb.off;
+    // 1. bucket counts
+    for (uint32_t i = lane; i < size; i += 32) atomicAdd(&cnt[(uint32_t)__ldg(src + i) >> bshift], 1u);
+    __syncwarp();
+    // 2. bucket bases: each lane owns kPer consecutive buckets
+    uint32_t c[kPer];
+    uint32_t t = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+      c[k] = cnt[lane * kPer + k];
+      t += c[k];
+    }
+    uint32_t tot;
+    uint32_t run = warp_excl_sum(t, &tot);
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+      base[lane * kPer + k] = run;
+      run += c[k];
+    }
+    __syncwarp();
+    // 3. every id to the next slot of its bucket (order inside a bucket is
+    //    settled below)
+    for (uint32_t i = lane; i < size; i += 32) {
+      const uint32_t v = (uint32_t)__ldg(src + i);
+      stage[atomicAdd(&base[v >> bshift], 1u)] = v;
+    }
+    __syncwarp();
+    // 4. insertion sort of each bucket [base - count, base); counts cleared
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+      const uint32_t n = c[k];
+      const uint32_t b0 = base[lane * kPer + k] - n;
+      for (uint32_t i = 1; i < n; ++i) {
+        const uint32_t key = stage[b0 + i];
+        uint32_t jj = i;
+        while (jj > 0 && stage[b0 + jj - 1] > key) {
+          stage[b0 + jj] = stage[b0 + jj - 1];
+          --jj;
+        }
+        stage[b0 + jj] = key;
+      }
+      cnt[lane * kPer + k] = 0;
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < size; i += 32) __stcs(out + jb.off + i, (int32_t)stage[i]);
+    __syncwarp();
+  }
+}
+
 __global__ void __launch_bounds__(kSmallThreads) k_sort_small(const Job* __restrict__ jobs,
                                                               const uint32_t* __restrict__ njobs_p,
                                                               int32_t* out, uint32_t idbits) {
@@ -88,6 +174,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_sort_small(const Job* __restr
   for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
     const Job jb = jobs[j];
     const uint32_t size = jb.size;
+    if (size <= kTinyCap) continue;  // CTA-uniform: k_sort_tiny's job
     // 1. count into buckets; each id's slot in its bucket is kept by index
     for (uint32_t i0 = 0; i0 < size; i0 += kSmallThreads * 8) {
       uint32_t v[8];
@@ -576,6 +663,8 @@ static qcp_status set_sort_attrs(const qcp_index* ix, size_t scatter_max) {
   if (attrs_device != ix->device) {
     QCP_CUDA(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(BucketSmem)));
+    QCP_CUDA(cudaFuncSetAttribute(k_sort_tiny, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(TinySmem)));
     QCP_CUDA(cudaFuncSetAttribute(k_win_sort<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(RankSmem<16>)));
     QCP_CUDA(cudaFuncSetAttribute(k_win_sort<17>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -615,9 +704,11 @@ qcp_status sort_small_slices(qcp_index* ix, Workspace* ws, uint32_t q, cudaStrea
   ws->sort_small_jobs = nsmall;
   ws->sort_msd_jobs = nbig;
   if (nsmall) {
+    k_sort_tiny<<<min((nsmall + kTinyWarps - 1) / kTinyWarps, sms * 4), kTinyWarps * 32, sizeof(TinySmem), s>>>(
+        small, ctr + kCtrJobs0, ws->out_ids, idbits);
     k_sort_small<<<min(nsmall, sms * 3), kSmallThreads, sizeof(BucketSmem), s>>>(small, ctr + kCtrJobs0,
                                                                                   ws->out_ids, idbits);
-    note_launch();
+    note_launch(2);
     QCP_TRY(check_launch("k_sort_small"));
   }
   *big_out = big;
@@ -754,7 +845,9 @@ qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void*
   QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t) * 2, s));
   k_classify<<<(q + 255) / 256, 256, 0, s>>>((const unsigned long long*)ws->offsets, q, small, ctr + kCtrJobs0,
                                              big, ctr + kCtrJobs1, nullptr);
+  k_sort_tiny<<<sms * 4, kTinyWarps * 32, sizeof(TinySmem), s>>>(small, ctr + kCtrJobs0, ws->out_ids, idbits);
   k_sort_small<<<sms * 3, kSmallThreads, sizeof(BucketSmem), s>>>(small, ctr + kCtrJobs0, ws->out_ids, idbits);
+  note_launch();
   k_tiles_per_job<<<(q + 255) / 256, 256, 0, s>>>(big, ctr + kCtrJobs1, q, tiles);
   note_launch(3);
   QCP_TRY(exclusive_scan<uint32_t>(tiles, tile_off, q, ctr + kCtrWork2, ix->pool, s, ws->scan_tmp,

@@ -85,6 +85,76 @@ __device__ __forceinline__ uint32_t test4(const Box<D>& b, const float* coords, 
   return m;
 }
 
+// Hit mask of objects g..g+3 of a leaf staged in shared memory: coordinate
+// run c of the leaf at s + c * F (lo0..lo(D-1), then hi.. for rectangles);
+// objects at or past `valid` (padding of the last leaf) never hit.
+template <int D, bool RECT>
+__device__ __forceinline__ uint32_t test4_staged(const Box<D>& b, const float* s, uint32_t F, uint32_t g,
+                                                 uint32_t valid) {
+  uint32_t m = 0xfu;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const float4 lo = *reinterpret_cast<const float4*>(s + (uint32_t)d * F + g);
+    float4 hi = lo;
+    if (RECT) hi = *reinterpret_cast<const float4*>(s + (uint32_t)(D + d) * F + g);
+    m &= (overlaps1(b.lo[d], b.hi[d], lo.x, hi.x) ? 1u : 0u) | (overlaps1(b.lo[d], b.hi[d], lo.y, hi.y) ? 2u : 0u) |
+         (overlaps1(b.lo[d], b.hi[d], lo.z, hi.z) ? 4u : 0u) | (overlaps1(b.lo[d], b.hi[d], lo.w, hi.w) ? 8u : 0u);
+  }
+  if (g + 4 > valid) m &= (g < valid) ? (1u << (valid - g)) - 1u : 0u;
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// Bulk copies (the TMA unit's non-tensor cp.async.bulk, global -> this CTA's
+// shared memory, no multicast) completing on an mbarrier.  Every wait is
+// bounded: after kBulkWaitCycles of clock it gives up and reports false.
+// ---------------------------------------------------------------------------
+constexpr long long kBulkWaitCycles = 4ll << 30;  // ~2 s at 2 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// generic-proxy accesses of this thread before async-proxy ones after
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for phase `parity` of `bar` to complete; false if it did not within
+// kBulkWaitCycles.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > kBulkWaitCycles) return false;
+  }
+  return true;
+}
+
 __device__ __forceinline__ uint32_t lane_lt_mask() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -11,10 +11,14 @@
 //                  in flight per SM;
 //   win_bits       id window of the per-query sort (2^win_bits ids per
 //                  bitmap), which trades partition fan-out against the
-//                  density of the window bitmaps.
+//                  density of the window bitmaps;
+//   leaf_prefetch  the leaf tile of the traversal's leaf passes: how many
+//                  partially covered leaves each warp keeps in flight in its
+//                  shared-memory ring (bulk copies), or none, which trades
+//                  latency hiding against CTAs per SM.
 // Search: coordinate descent -- fan-out first (every candidate built and
-// queried with default knobs), then blocks_per_sm, then win_bits, each at the
-// best values found so far.  A trial is the median of `repeats` timed
+// queried with default knobs), then blocks_per_sm, then win_bits, then
+// leaf_prefetch, each at the best values found so far.  A trial is the median of `repeats` timed
 // batches after one untimed batch, timed with CUDA events on the call's
 // stream, sorted output left on the device.
 #include <algorithm>
@@ -31,7 +35,7 @@ struct Trial {
 };
 
 Trial time_batch(qcp_index* ix, const float* d_boxes, uint32_t q, cudaStream_t s, uint32_t bps, uint32_t wb,
-                 uint32_t repeats, cudaEvent_t e0, cudaEvent_t e1) {
+                 uint32_t lp, uint32_t repeats, cudaEvent_t e0, cudaEvent_t e1) {
   Trial tr;
   qcp_query_opts o;
   memset(&o, 0, sizeof(o));
@@ -40,6 +44,7 @@ Trial time_batch(qcp_index* ix, const float* d_boxes, uint32_t q, cudaStream_t s
   o.stream = s;
   o.blocks_per_sm = bps;
   o.win_bits = wb;
+  o.leaf_prefetch = lp;
   std::vector<float> ms;
   for (uint32_t r = 0; r <= repeats; ++r) {
     qcp_result res;
@@ -88,18 +93,19 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
       st = qcp::cuda_status(cudaGetLastError(), "qcp_autotune setup");
       break;
     }
-    auto record = [&](uint32_t f, uint32_t b, uint32_t w, float ms) {
+    auto record = [&](uint32_t f, uint32_t b, uint32_t w, uint32_t lp, float ms) {
       if (out->trials < QCP_TUNE_MAX_TRIALS) {
         out->trial_fanout[out->trials] = f;
         out->trial_blocks_per_sm[out->trials] = b;
         out->trial_win_bits[out->trials] = w;
+        out->trial_leaf_prefetch[out->trials] = lp;
         out->trial_ms[out->trials] = ms;
         ++out->trials;
       }
     };
     // 1. fan-out, default knobs
     const uint32_t fanouts[] = {64, 128, 256};
-    uint32_t best_f = 0, best_b = 8, best_w = qcp::kDefaultWinBits;
+    uint32_t best_f = 0, best_b = 8, best_w = qcp::kDefaultWinBits, best_lp = qcp::kDefaultLeafRing;
     float best = 0.f, best_build = 0.f;
     for (uint32_t f : fanouts) {
       bo.fanout = f;
@@ -109,13 +115,13 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
       const float build_ms =
           std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
       if (st != QCP_OK) break;
-      const Trial tr = time_batch(ix, (const float*)d_boxes, q, s, best_b, best_w, repeats, e0, e1);
+      const Trial tr = time_batch(ix, (const float*)d_boxes, q, s, best_b, best_w, best_lp, repeats, e0, e1);
       if (tr.st != QCP_OK) {
         st = tr.st;
         qcp_index_free(ix);
         break;
       }
-      record(f, best_b, best_w, tr.ms);
+      record(f, best_b, best_w, best_lp, tr.ms);
       if (!best_ix || tr.ms < best) {
         if (best_ix) qcp_index_free(best_ix);
         best_ix = ix;
@@ -129,9 +135,9 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
     if (st != QCP_OK) break;
     // 2. blocks per SM, then 3. sort window bits, at the best so far
     for (uint32_t b : {4u, 16u}) {
-      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, b, best_w, repeats, e0, e1);
+      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, b, best_w, best_lp, repeats, e0, e1);
       if ((st = tr.st) != QCP_OK) break;
-      record(best_f, b, best_w, tr.ms);
+      record(best_f, b, best_w, best_lp, tr.ms);
       if (tr.ms < best) {
         best = tr.ms;
         best_b = b;
@@ -141,16 +147,28 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
     const uint32_t first_w = best_w;
     for (uint32_t w : {16u, 17u, 18u}) {
       if (w == first_w) continue;
-      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, best_b, w, repeats, e0, e1);
+      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, best_b, w, best_lp, repeats, e0, e1);
       if ((st = tr.st) != QCP_OK) break;
-      record(best_f, best_b, w, tr.ms);
+      record(best_f, best_b, w, best_lp, tr.ms);
       if (tr.ms < best) {
         best = tr.ms;
         best_w = w;
       }
     }
     if (st != QCP_OK) break;
+    // 4. leaf tile: no ring (1), or 3 buffers per warp instead of 2
+    for (uint32_t lp : {1u, 3u}) {
+      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, best_b, best_w, lp, repeats, e0, e1);
+      if ((st = tr.st) != QCP_OK) break;
+      record(best_f, best_b, best_w, lp, tr.ms);
+      if (tr.ms < best) {
+        best = tr.ms;
+        best_lp = lp;
+      }
+    }
+    if (st != QCP_OK) break;
     out->fanout = best_f;
+    out->leaf_prefetch = best_lp;
     out->blocks_per_sm = best_b;
     out->win_bits = best_w;
     out->best_ms = best;

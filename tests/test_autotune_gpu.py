@@ -1,7 +1,8 @@
 """Autotuner (qcp_autotune) and the query knobs it sets.
 
 The knobs change how the work is laid out on the GPU, never the result: a
-search with any blocks_per_sm / win_bits must return the oracle's ids.  The
+search with any blocks_per_sm / win_bits / leaf_prefetch must return the
+oracle's ids.  The
 tuner must pick from its candidate sets, record every trial, and report the
 time of the trial it chose.  Needs a GPU."""
 from __future__ import annotations
@@ -22,12 +23,48 @@ def data(workloads, oracle):
     return objs, boxes, want_offs, want_ids
 
 
-@pytest.mark.parametrize("bps,wb", [(4, 16), (16, 17), (32, 12), (1, 18)])
-def test_knobs_keep_hits_exact(qcp, data, bps, wb):
+@pytest.mark.parametrize("bps,wb,lp", [(4, 16, 1), (16, 17, 2), (32, 12, 3), (1, 18, 4), (8, 17, 1), (8, 16, 3)])
+def test_knobs_keep_hits_exact(qcp, data, bps, wb, lp):
     objs, boxes, want_offs, want_ids = data
     with qcp.Index.build(objs, fanout=64) as ix:
-        res = ix.search(boxes, blocks_per_sm=bps, win_bits=wb)
+        res = ix.search(boxes, blocks_per_sm=bps, win_bits=wb, leaf_prefetch=lp)
         assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
+        assert np.array_equal(ix.counts(boxes, leaf_prefetch=lp), np.diff(want_offs))
+
+
+@pytest.mark.parametrize("fanout", [32, 128, 256])
+@pytest.mark.parametrize("lp", [1, 2, 4])
+def test_leaf_tile_at_every_fanout(qcp, data, fanout, lp):
+    """The leaf prefetch ring (bulk copies of partially covered leaves into
+    shared memory) against direct loads, at fan-outs whose leaves are 128 B
+    to 1 KB per coordinate run."""
+    objs, boxes, want_offs, want_ids = data
+    with qcp.Index.build(objs, fanout=fanout) as ix:
+        res = ix.search(boxes[:150], leaf_prefetch=lp)
+        n = int(want_offs[150])
+        assert_same_hits(res.offsets, res.ids, want_offs[:151], want_ids[:n])
+
+
+@pytest.mark.parametrize("lp", [1, 2, 3])
+def test_leaf_tile_rectangles_and_2d(qcp, oracle, cases, lp):
+    """Rectangles (lo and hi runs per leaf) and 2-D points through the ring."""
+    rng = np.random.default_rng(81)
+    lo = rng.random((40000, 8), dtype=np.float32)
+    hi = (lo + rng.exponential(0.05, (40000, 8)).astype(np.float32)).astype(np.float32)
+    objs = np.ascontiguousarray(np.concatenate([lo, hi], 1))
+    c = rng.random((120, 8), dtype=np.float32)
+    sd = rng.uniform(0.3, 0.7, (120, 8)).astype(np.float32) / 2
+    boxes = np.ascontiguousarray(np.concatenate([c - sd, c + sd], 1), dtype=np.float32)
+    want_offs, want_ids = oracle.ids(objs, 8, True, boxes)
+    for fanout in (32, 64):
+        with qcp.Index.build(objs, is_rect=True, fanout=fanout) as ix:
+            res = ix.search(boxes, leaf_prefetch=lp)
+            assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
+    objs2, boxes2, _ = cases.COUNT_CASES["u2"]()
+    o2, i2 = oracle.ids(objs2, 2, False, boxes2)
+    with qcp.Index.build(objs2) as ix:
+        res = ix.search(boxes2, leaf_prefetch=lp)
+        assert_same_hits(res.offsets, res.ids, o2, i2)
 
 
 def test_autotune_choice_and_trials(qcp, data):
@@ -36,11 +73,13 @@ def test_autotune_choice_and_trials(qcp, data):
     assert r["fanout"] in (64, 128, 256)
     assert r["blocks_per_sm"] in (4, 8, 16)
     assert r["win_bits"] in (16, 17, 18)
-    assert len(r["trials"]) == 7  # 3 fan-outs, 2 more grids, 2 more windows
+    assert r["leaf_prefetch"] in (1, 2, 3)
+    assert len(r["trials"]) == 9  # 3 fan-outs, 2 more grids, 2 more windows, 2 more leaf tiles
     assert r["best_ms"] == pytest.approx(min(t["ms"] for t in r["trials"]))
     chosen = [t for t in r["trials"] if t["ms"] == r["best_ms"]][0]
-    assert (chosen["fanout"], chosen["blocks_per_sm"], chosen["win_bits"]) == \
-        (r["fanout"], r["blocks_per_sm"], r["win_bits"])
+    assert (chosen["fanout"], chosen["blocks_per_sm"], chosen["win_bits"], chosen["leaf_prefetch"]) == \
+        (r["fanout"], r["blocks_per_sm"], r["win_bits"], r["leaf_prefetch"])
     with qcp.Index.build(objs, fanout=r["fanout"]) as ix:
-        res = ix.search(boxes, blocks_per_sm=r["blocks_per_sm"], win_bits=r["win_bits"])
+        res = ix.search(boxes, blocks_per_sm=r["blocks_per_sm"], win_bits=r["win_bits"],
+                        leaf_prefetch=r["leaf_prefetch"])
         assert_same_hits(res.offsets, res.ids, want_offs, want_ids)

@@ -196,3 +196,30 @@ def test_large_result_slices(qcp, oracle, workloads, n):
         for algo in ["batched", "plain"]:
             res = ix.search(boxes, algo=algo)
             assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
+
+
+def test_slice_sizes_at_every_sort_boundary(qcp, oracle):
+    """Slices of exactly k ids around the sort's size classes: one warp per
+    slice up to 1,024 ids, one CTA up to 8,192, id windows above.  Points
+    sit on a line in random id order, so a box [x0, x1] selects an exact,
+    randomly numbered run of them."""
+    n = 200_000
+    rng = np.random.default_rng(1024)
+    order = rng.permutation(n)
+    objs = np.zeros((n, 3), np.float32)
+    objs[order, 0] = ((np.arange(n) + 0.5) / n).astype(np.float32)
+    objs[:, 1:] = 0.5
+    sizes = [1, 2, 31, 32, 33, 255, 256, 257, 1023, 1024, 1025, 4096, 8191, 8192, 8193, 20000, 131073]
+    boxes = []
+    for k in sizes:
+        start = int(rng.integers(0, n - k))
+        lo = np.float32((start + 0.25) / n)
+        hi = np.float32((start + k - 0.25) / n)
+        boxes.append([lo, 0.4, 0.4, hi, 0.6, 0.6])
+    boxes = np.asarray(boxes * 3, np.float32)  # every size three times in one batch
+    want_offs, want_ids = oracle.ids(objs, 3, False, boxes)
+    assert list(np.diff(want_offs)[:len(sizes)]) == sizes
+    with qcp.Index.build(objs) as ix:
+        for algo in ["batched", "plain"]:
+            res = ix.search(boxes, algo=algo)
+            assert_same_hits(res.offsets, res.ids, want_offs, want_ids, boxes)
