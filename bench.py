@@ -261,17 +261,19 @@ def run_ours(args, rank, world, local):
 
     # ---- autotune on a separate query sample of the same distribution -------
     knobs = {"fanout": args.fanout, "blocks_per_sm": args.blocks_per_sm, "win_bits": args.win_bits,
-             "leaf_prefetch": args.leaf_prefetch}
+             "leaf_prefetch": args.leaf_prefetch, "lanes_per_item": args.lanes_per_item}
     tune = None
     if args.algo == "batched" and not args.no_tune:
         sample = tune_sample(W, args.workload, w)
         tune = qcp.autotune(w.objs, sample, is_rect=w.is_rect, dims=w.dims, repeats=2)
-        knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch")}
+        knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch", "lanes_per_item")}
     args.fanout = knobs["fanout"]
 
     t0 = time.perf_counter()
     ix = qcp.Index.build(d_objs, dims=w.dims, n=w.n, is_rect=w.is_rect, fanout=args.fanout, stream=sp)
     build_ms = (time.perf_counter() - t0) * 1e3
+    hbm, peak_kind = peaks()
+    build_plan = time_build_plan(qcp, w, args.fanout, d_objs, sp, hbm, peak_kind)
     info = ix.info()
 
     def barrier():
@@ -288,7 +290,7 @@ def run_ours(args, rank, world, local):
     def step_device(algo, timing):
         r = ix.search(d_boxes, q=Q, algo=algo, result_mem=qcp.MEM_DEVICE, stream=sp, timing=timing,
                       blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
-                    leaf_prefetch=knobs["leaf_prefetch"])
+                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"])
         hits = r.total_hits
         r.release()
         return hits
@@ -335,7 +337,7 @@ def run_ours(args, rank, world, local):
     # ---- parity of the timed batch (after the timed region) -----------------
     res = ix.search(d_boxes, q=Q, algo=args.algo, result_mem=qcp.MEM_DEVICE, stream=sp,
                     blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
-                    leaf_prefetch=knobs["leaf_prefetch"])
+                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"])
     got_counts, nchecked, fail = verify_result(res, Q, d_objs, d_boxes, w.dims, w.is_rect)
     res.release()
     parity = {"ids_checked": int(nchecked), "slices_ascending_and_in_box": fail is None}
@@ -361,7 +363,7 @@ def run_ours(args, rank, world, local):
         def step_unsorted(algo):
             r = ix.search(d_boxes, q=Q, algo=algo, sort=False, result_mem=qcp.MEM_DEVICE, stream=sp,
                           blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
-                    leaf_prefetch=knobs["leaf_prefetch"])
+                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"])
             r.release()
 
         plain = qps_of(lambda: step_device("plain", False))
@@ -385,7 +387,7 @@ def run_ours(args, rank, world, local):
     def step_host(st):
         r = ix.search(h_np, algo=args.algo, result_mem=qcp.MEM_HOST, stream=st.cuda_stream, copy=False,
                       blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
-                    leaf_prefetch=knobs["leaf_prefetch"])
+                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"])
         nb = (Q + 1) * 8 + r.total_hits * 4
         r.release()
         return nb
@@ -463,7 +465,7 @@ def run_ours(args, rank, world, local):
         plan_out = {}
         # (a) the timed batch itself through one plan
         with qcp.Plan(ix, Q, int(stats["hits"] * 1.05) + 1024, blocks_per_sm=knobs["blocks_per_sm"],
-                      win_bits=knobs["win_bits"], leaf_prefetch=knobs["leaf_prefetch"]) as plan:
+                      win_bits=knobs["win_bits"], leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"]) as plan:
             plan.run_device(d_boxes, q=Q, stream=sp)
             torch.cuda.synchronize()
             e_a = torch.cuda.Event(enable_timing=True)
@@ -515,7 +517,7 @@ def run_ours(args, rank, world, local):
             for _ in range(args.steps):
                 ix.search(h_np, algo="hybrid", result_mem=qcp.MEM_DEVICE, stream=sp, handoff_level=h,
                           blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
-                    leaf_prefetch=knobs["leaf_prefetch"]).release()
+                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"]).release()
             e_b.record(stream)
             e_b.synchronize()
             hm = e_a.elapsed_time(e_b) / args.steps
@@ -598,11 +600,12 @@ def run_ours(args, rank, world, local):
             "fanout": args.fanout, "blocks_per_sm": knobs["blocks_per_sm"] or 8,
             "win_bits": knobs["win_bits"] or 17,
             "leaf_prefetch": knobs["leaf_prefetch"] or 2,
+            "lanes_per_item": knobs["lanes_per_item"] or 32,
             "tuned": None if tune is None else {"sample_queries": 2000, "best_ms": round(tune["best_ms"], 3),
                                                 "trial_fields": ["fanout", "blocks_per_sm", "win_bits",
-                                                                 "leaf_prefetch", "ms"],
+                                                                 "leaf_prefetch", "lanes_per_item", "ms"],
                                                 "trials": [[t["fanout"], t["blocks_per_sm"], t["win_bits"],
-                                                            t["leaf_prefetch"],
+                                                            t["leaf_prefetch"], t["lanes_per_item"],
                                                             round(t["ms"], 3)] for t in tune["trials"]]},
             "algo": args.algo, "queries_per_step_per_gpu": Q,
             "n_objects": w.n, "key": f"hilbert {info['key_bits']} bits/dim",
@@ -615,6 +618,7 @@ def run_ours(args, rank, world, local):
                              "p99": round(float(np.percentile(lat, 99)), 3)},
         "hits_per_step": int(stats["hits"]),
         "build_ms": round(build_ms, 2),
+        "build_plan": build_plan,
         "phase_ms_per_step": {k: round(v / args.steps, 4) for k, v in phase.items()},
         "work_per_step": {k: stats[k] for k in ["leaf_items", "leaves_covered", "leaves_partial",
                                                  "objects_covered", "sort_small_jobs", "sort_msd_jobs",
@@ -648,6 +652,45 @@ def run_ours(args, rank, world, local):
         sys.exit(3)
 
 
+def time_build_plan(qcp, w, fanout, d_objs, sp, hbm, peak_kind, runs=5):
+    """Device time of the captured build (qcp_build_plan_run, one graph
+    launch, objects already in the plan's input buffer) and its HBM
+    roofline with the algorithmic bytes of the build: keys N*(4D + 12) (read
+    the coordinates, write key and id), sort 4*N*12*2 (four passes of 16-bit
+    digits over key + id, read and write), packing N*(4D' + 4) read plus
+    the written index (coordinates, ids, every MBR level); D' = D or 2D."""
+    import torch
+    stream = torch.cuda.current_stream(d_objs.device)
+    with qcp.BuildPlan(w.n, w.dims, is_rect=w.is_rect, fanout=fanout, key_bits=w.key_bits) as plan:
+        ix = plan.run(d_objs, stream=sp)  # objects into the plan's input buffer
+        info = ix.info()
+        for _ in range(2):
+            plan.run(None, stream=sp)
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(runs):
+            e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e_a.record(stream)
+            plan.run(None, stream=sp)
+            e_b.record(stream)
+            e_b.synchronize()
+            ms.append(e_a.elapsed_time(e_b))
+    n, d = w.n, w.dims
+    nc = 2 * d if w.is_rect else d
+    F = fanout
+    npad = -(-n // F) * F
+    mbr_bytes = sum(-(-k // F) * F * 2 * d * 4 for k in info["level_nodes"])
+    algo = n * (4 * d + 12) + 4 * n * 12 * 2 + n * (4 * nc + 4) + npad * (4 * nc + 4) + mbr_bytes
+    best = float(np.median(ms))
+    gbs = algo / (best / 1e3) / 1e9
+    return {"ms": round(best, 3), "runs_ms": [round(x, 3) for x in ms],
+            "what": "qcp_build_plan_run: keys, radix sort, packing, MBR levels replayed as one CUDA graph, "
+                    "objects resident on the device",
+            "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
+                         "frac": round(gbs / hbm, 4), "peak_kind": peak_kind,
+                         "algorithmic_bytes": int(algo)}}
+
+
 def measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind):
     """A compact line for another workload on the same GPU: tuned knobs,
     device-resident queries/s, the plain traversal, host-buffer e2e, the
@@ -658,11 +701,11 @@ def measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind):
     stream = torch.cuda.current_stream(dev)
     d_objs = torch.from_numpy(w.objs).to(dev)
     d_boxes = torch.from_numpy(boxes).to(dev)
-    knobs = {"fanout": 128, "blocks_per_sm": 0, "win_bits": 0, "leaf_prefetch": 0}
+    knobs = {"fanout": 128, "blocks_per_sm": 0, "win_bits": 0, "leaf_prefetch": 0, "lanes_per_item": 0}
     tune = None
     if not args.no_tune:
         tune = qcp.autotune(w.objs, tune_sample(W, name, w), is_rect=w.is_rect, dims=w.dims, repeats=2)
-        knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch")}
+        knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch", "lanes_per_item")}
     build = dict(fanout=knobs["fanout"], dims=w.dims, n=w.n, is_rect=w.is_rect, key_bits=w.key_bits, stream=sp)
     qcp.Index.build(d_objs, **build).close()  # warm-up build
     torch.cuda.synchronize()
@@ -672,10 +715,11 @@ def measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind):
         ixb = qcp.Index.build(d_objs, **build)
         build_ms.append((time.perf_counter() - t0) * 1e3)
         ixb.close()
+    build_plan = time_build_plan(qcp, w, knobs["fanout"], d_objs, sp, hbm, peak_kind)
     ix = qcp.Index.build(d_objs, **build)
     info = ix.info()
     kq = dict(blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
-                    leaf_prefetch=knobs["leaf_prefetch"])
+                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"])
 
     def step(algo, timing=False):
         r = ix.search(d_boxes, q=Q, algo=algo, result_mem=qcp.MEM_DEVICE, stream=sp, timing=timing, **kq)
@@ -746,7 +790,7 @@ def measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind):
            "steps": args.steps, "warmup": args.warmup, "hits_per_step": int(stats["hits"]),
            "knobs": knobs, "key": f"hilbert {info['key_bits']} bits/dim", "levels": info["levels"],
            "tuned": None if tune is None else [[t["fanout"], t["blocks_per_sm"], t["win_bits"], t["leaf_prefetch"],
-                                                round(t["ms"], 3)]
+                                                t["lanes_per_item"], round(t["ms"], 3)]
                                                for t in tune["trials"]],
            "phase_ms_per_step": {k: round(v / args.steps, 4) for k, v in phase.items()},
            "roofline": roof,
@@ -756,6 +800,7 @@ def measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind):
                    "d2h_bytes_per_step": int(d2h)},
            "build_ms": {"min": round(min(build_ms), 2), "runs": [round(x, 2) for x in build_ms],
                         "what": "qcp_index_build from device-resident objects, host wall clock, allocation included"},
+           "build_plan": build_plan,
            "parity": parity, "clocks": clk}
     if cpu is not None:
         out["cpu_baseline"] = cpu
@@ -873,6 +918,8 @@ def main():
     ap.add_argument("--fanout", type=int, default=128)
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="traversal blocks per SM with --no-tune (0: default)")
     ap.add_argument("--win-bits", type=int, default=0, help="sort window bits with --no-tune (0: default)")
+    ap.add_argument("--lanes-per-item", type=int, default=0,
+                    help="lanes per (query, node) item of the level expansion with --no-tune (0: 32)")
     ap.add_argument("--leaf-prefetch", type=int, default=0,
                     help="leaf prefetch buffers per warp with --no-tune (0: default 2, 1: none)")
     ap.add_argument("--plain-steps", type=int, default=2)

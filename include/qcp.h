@@ -139,6 +139,10 @@ typedef struct qcp_query_opts {
    * itself), 2..4 = that many buffers (fewer where shared memory is short).
    * qcp_autotune picks it. */
   uint32_t leaf_prefetch;
+  /* Queries per warp of the batched traversal's level expansion: lanes
+   * that share one (query, node) item, 32 (default, 0), 16 or 8 (two or
+   * four items per warp at once).  qcp_autotune picks it. */
+  uint32_t lanes_per_item;
 } qcp_query_opts;
 
 /* flags: record CUDA events around every phase of the call; the times are
@@ -258,11 +262,12 @@ qcp_status qcp_query_counts_noalloc(qcp_index* index, const float* d_boxes, uint
                                     uint64_t* d_counts, void* stream);
 
 /* Autotuner: picks the build fan-out and the query knobs (blocks_per_sm,
- * win_bits, leaf_prefetch) for a data set and a sample of its queries by
- * timing trials on the current device: every fan-out in {64, 128, 256} is
- * built and queried with the default knobs, then blocks_per_sm in {4, 8,
- * 16}, win_bits in {16, 17, 18} and leaf_prefetch in {1, 2, 3} are tried one
- * after the other at the best fan-out (coordinate descent); each trial is the median of `repeats` timed batches of the
+ * win_bits, leaf_prefetch, lanes_per_item) for a data set and a sample of
+ * its queries by timing trials on the current device: every fan-out in {64,
+ * 128, 256} is built and queried with the default knobs, then blocks_per_sm
+ * in {4, 8, 16}, win_bits in {16, 17, 18}, leaf_prefetch in {1, 2, 3} and
+ * lanes_per_item in {8, 16, 32} are tried one after the other at the best
+ * fan-out (coordinate descent); each trial is the median of `repeats` timed batches of the
  * sample (sorted output) after one untimed batch.  objs and boxes are host
  * memory as for qcp_index_build / qcp_query_batch; `base` supplies the key
  * mode, key bits and stream (its fanout is ignored).  The reference fixes
@@ -282,6 +287,8 @@ typedef struct qcp_tune_result {
   float trial_ms[QCP_TUNE_MAX_TRIALS];
   uint32_t leaf_prefetch;     /* best qcp_query_opts.leaf_prefetch */
   uint32_t trial_leaf_prefetch[QCP_TUNE_MAX_TRIALS];
+  uint32_t lanes_per_item;    /* best qcp_query_opts.lanes_per_item */
+  uint32_t trial_lanes_per_item[QCP_TUNE_MAX_TRIALS];
 } qcp_tune_result;
 
 qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims, uint32_t is_rect, const float* boxes,
@@ -294,7 +301,8 @@ qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims, uint32_t i
  * creation (device memory for max_queries boxes, the frontier, max_hits ids
  * twice, the sort's tables) so every phase runs from device-resident counts,
  * and one graph launch replaces its ~20 kernel launches and 3 host round
- * trips.  opts: blocks_per_sm, win_bits, leaf_prefetch and unsorted are used (algo must be
+ * trips.  opts: blocks_per_sm, win_bits, leaf_prefetch, lanes_per_item and
+ * unsorted are used (algo must be
  * batched; NULL = defaults).  qcp_plan_create runs the pipeline once on an
  * empty batch before capturing it.
  *

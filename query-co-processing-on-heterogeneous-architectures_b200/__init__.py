@@ -58,7 +58,7 @@ class QueryOpts(ctypes.Structure):
                 ("stream", ctypes.c_void_p), ("flags", ctypes.c_uint32),
                 ("blocks_per_sm", ctypes.c_uint32), ("win_bits", ctypes.c_uint32),
                 ("cpu_threads", ctypes.c_uint32), ("handoff_level", ctypes.c_uint32),
-                ("leaf_prefetch", ctypes.c_uint32)]
+                ("leaf_prefetch", ctypes.c_uint32), ("lanes_per_item", ctypes.c_uint32)]
 
 
 QUERY_TIMING = 1
@@ -120,7 +120,9 @@ class TuneResult(ctypes.Structure):
                 ("trial_win_bits", ctypes.c_uint32 * TUNE_MAX_TRIALS),
                 ("trial_ms", ctypes.c_float * TUNE_MAX_TRIALS),
                 ("leaf_prefetch", ctypes.c_uint32),
-                ("trial_leaf_prefetch", ctypes.c_uint32 * TUNE_MAX_TRIALS)]
+                ("trial_leaf_prefetch", ctypes.c_uint32 * TUNE_MAX_TRIALS),
+                ("lanes_per_item", ctypes.c_uint32),
+                ("trial_lanes_per_item", ctypes.c_uint32 * TUNE_MAX_TRIALS)]
 
 
 class Result(ctypes.Structure):
@@ -317,16 +319,16 @@ class Index:
 
     # -- queries --------------------------------------------------------------
     def _opts(self, algo, boxes_mem, result_mem, sort, stream, timing=False, blocks_per_sm=0, win_bits=0,
-              cpu_threads=0, handoff_level=0, leaf_prefetch=0):
+              cpu_threads=0, handoff_level=0, leaf_prefetch=0, lanes_per_item=0):
         a = {"batched": ALGO_BATCHED, "plain": ALGO_PLAIN, "hybrid": ALGO_HYBRID}.get(algo, algo)
         return QueryOpts(a, boxes_mem, result_mem, 0 if sort else 1, ctypes.c_void_p(stream or None),
                          QUERY_TIMING if timing else 0, blocks_per_sm, win_bits, cpu_threads, handoff_level,
-                         leaf_prefetch)
+                         leaf_prefetch, lanes_per_item)
 
     def search(self, boxes, algo="batched", sort: bool = True, result_mem: int = MEM_HOST,
                q: int | None = None, stream: int = 0, timing: bool = False,
                copy: bool = True, blocks_per_sm: int = 0, win_bits: int = 0, cpu_threads: int = 0,
-               handoff_level: int = 0, leaf_prefetch: int = 0) -> SearchResult:
+               handoff_level: int = 0, leaf_prefetch: int = 0, lanes_per_item: int = 0) -> SearchResult:
         """Run a batch of box queries.  Host numpy boxes (q x 2D) or a CUDA
         tensor/pointer (then pass q).  Host results are copied into numpy
         arrays (copy=False: numpy views of the library's pinned result arena,
@@ -341,7 +343,7 @@ class Index:
                 raise ValueError("device boxes need q")
             b, nq, ptr, bmem = boxes, q, ctypes.c_void_p(_device_ptr(boxes)), MEM_DEVICE
         opts = self._opts(algo, bmem, result_mem, sort, stream, timing, blocks_per_sm, win_bits, cpu_threads,
-                          handoff_level, leaf_prefetch)
+                          handoff_level, leaf_prefetch, lanes_per_item)
         r = Result()
         _check(lib.qcp_query_batch(self._h, ptr, nq, ctypes.byref(opts), ctypes.byref(r)))
         if result_mem == MEM_HOST and not copy:
@@ -367,7 +369,7 @@ class Index:
         return SearchResult(r.offsets, r.ids, int(r.total_hits), MEM_DEVICE, raw=r)
 
     def counts(self, boxes, algo="batched", q: int | None = None, stream: int = 0,
-               leaf_prefetch: int = 0) -> np.ndarray:
+               leaf_prefetch: int = 0, lanes_per_item: int = 0) -> np.ndarray:
         lib = load_library()
         if isinstance(boxes, np.ndarray):
             b = np.ascontiguousarray(boxes, dtype=np.float32).reshape(-1, 2 * self.dims)
@@ -375,7 +377,8 @@ class Index:
         else:
             b, nq, ptr, bmem = boxes, q, ctypes.c_void_p(_device_ptr(boxes)), MEM_DEVICE
         out = np.zeros(nq, np.uint64)
-        opts = self._opts(algo, bmem, MEM_HOST, True, stream, leaf_prefetch=leaf_prefetch)
+        opts = self._opts(algo, bmem, MEM_HOST, True, stream, leaf_prefetch=leaf_prefetch,
+                          lanes_per_item=lanes_per_item)
         _check(lib.qcp_query_counts(self._h, ptr, nq, ctypes.byref(opts), _ptr(out)))
         return out
 
@@ -433,11 +436,11 @@ class Plan:
     offsets and ids; run_device() the plan's device pointers."""
 
     def __init__(self, index: "Index", max_queries: int, max_hits: int, sort: bool = True,
-                 blocks_per_sm: int = 0, win_bits: int = 0, leaf_prefetch: int = 0):
+                 blocks_per_sm: int = 0, win_bits: int = 0, leaf_prefetch: int = 0, lanes_per_item: int = 0):
         self.index = index
         self._h = ctypes.c_void_p()
         opts = index._opts("batched", MEM_HOST, MEM_DEVICE, sort, 0, False, blocks_per_sm, win_bits,
-                           leaf_prefetch=leaf_prefetch)
+                           leaf_prefetch=leaf_prefetch, lanes_per_item=lanes_per_item)
         _check(load_library().qcp_plan_create(index._h, max_queries, max_hits, ctypes.byref(opts),
                                               ctypes.byref(self._h)))
 
@@ -536,10 +539,11 @@ def autotune(objs, boxes, is_rect: bool = False, dims: int | None = None, key_mo
                                        ctypes.byref(bo), repeats, ctypes.byref(r)))
     n = r.trials
     return {"fanout": r.fanout, "blocks_per_sm": r.blocks_per_sm, "win_bits": r.win_bits,
-            "leaf_prefetch": r.leaf_prefetch, "best_ms": r.best_ms, "build_ms": r.build_ms,
+            "leaf_prefetch": r.leaf_prefetch, "lanes_per_item": r.lanes_per_item,
+            "best_ms": r.best_ms, "build_ms": r.build_ms,
             "trials": [{"fanout": r.trial_fanout[i], "blocks_per_sm": r.trial_blocks_per_sm[i],
                         "win_bits": r.trial_win_bits[i], "leaf_prefetch": r.trial_leaf_prefetch[i],
-                        "ms": r.trial_ms[i]} for i in range(n)]}
+                        "lanes_per_item": r.trial_lanes_per_item[i], "ms": r.trial_ms[i]} for i in range(n)]}
 
 
 def last_stats() -> dict:

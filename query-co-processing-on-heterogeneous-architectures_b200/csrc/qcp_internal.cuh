@@ -116,6 +116,7 @@ struct Workspace {
   uint32_t blocks_per_sm = 8;    // traversal grid = SMs x this, this call
   uint32_t win_bits = 18;        // sort window, this call
   uint32_t leaf_ring = 2;        // leaf prefetch buffers per warp, this call (< 2: none)
+  uint32_t lanes_per_item = 32;  // lanes of k_expand per (query, node) item, this call
   // CPU + GPU co-processing (QCP_ALGO_HYBRID) of this call
   bool hybrid = false;
   uint32_t cpu_threads = 0, handoff_level = 1;
@@ -369,6 +370,9 @@ inline uint32_t leaf_ring_of(uint32_t knob) {
   if (knob == 1) return 0;
   return knob > 4 ? 4u : knob;
 }
+// Lanes per (query, node) item of the level expansion for a
+// qcp_query_opts.lanes_per_item value (0 = 32; 8, 16 or 32).
+inline uint32_t lanes_per_item_of(uint32_t knob) { return (knob == 8 || knob == 16) ? knob : 32u; }
 // Largest window count whose per-window counts the write pass gathers.
 constexpr uint32_t kHistMaxG = 256;
 // Default log2 of the per-query sort's id windows (qcp_query_opts.win_bits).

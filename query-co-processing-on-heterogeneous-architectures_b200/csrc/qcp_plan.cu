@@ -80,6 +80,7 @@ extern "C" qcp_status qcp_plan_create(qcp_index* ix, uint32_t max_queries, uint6
   ws->blocks_per_sm = (opts && opts->blocks_per_sm) ? (opts->blocks_per_sm > 32 ? 32u : opts->blocks_per_sm) : 8u;
   ws->win_bits = (opts && opts->win_bits) ? (opts->win_bits < 12 ? 12u : opts->win_bits) : kDefaultWinBits;
   ws->leaf_ring = leaf_ring_of(opts ? opts->leaf_prefetch : 0u);
+  ws->lanes_per_item = lanes_per_item_of(opts ? opts->lanes_per_item : 0u);
   qcp_status st = QCP_OK;
   do {
     const size_t row = 2 * (size_t)ix->dims;

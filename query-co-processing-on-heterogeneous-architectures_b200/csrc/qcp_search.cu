@@ -43,7 +43,11 @@ __global__ void k_init_items(uint2* items, uint32_t q, uint32_t node, uint32_t* 
   if (blockIdx.x == 0 && threadIdx.x == 0) *count = q;
 }
 
-template <int D>
+// LPI lanes per (query, node) item (32, 16 or 8: 1, 2 or 4 items per warp
+// at once); each group tests its item's children LPI at a time, compacts the
+// overlapping ones with the group's part of one warp ballot and reserves
+// their slots with one atomic per group and round.
+template <int D, int LPI>
 __global__ void __launch_bounds__(256) k_expand(const float* __restrict__ boxes,
                                                 const uint2* __restrict__ in,
                                                 const uint32_t* __restrict__ in_count,
@@ -51,33 +55,45 @@ __global__ void __launch_bounds__(256) k_expand(const float* __restrict__ boxes,
                                                 uint64_t out_cap, const float* __restrict__ child_mbr,
                                                 uint64_t nchild, uint64_t child_pad, uint32_t fanout,
                                                 uint32_t* overflow, uint32_t* need) {
+  constexpr uint32_t kGroups = 32 / LPI;
+  constexpr uint32_t kGroupMask = LPI == 32 ? 0xffffffffu : ((1u << LPI) - 1u);
   const uint32_t lane = threadIdx.x & 31;
+  const uint32_t grp = lane / LPI, gl = lane % LPI;
   // the counter keeps counting past the capacity when a level overflowed
   const uint32_t nin = (uint32_t)min((uint64_t)*in_count, out_cap);
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nin; i += warps) {
-    const uint2 it = in[i];
-    const Box<D> b = load_box<D>(boxes, it.x);
-    const uint64_t c0 = (uint64_t)it.y * fanout;
-    const uint64_t c1 = (c0 + fanout < nchild) ? c0 + fanout : nchild;
-    for (uint64_t cb = c0; cb < c1; cb += 32) {
-      const uint64_t c = cb + lane;
+  const uint32_t rounds = (fanout + LPI - 1) / LPI;  // warp-uniform
+  for (uint32_t i0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kGroups; i0 < nin; i0 += warps * kGroups) {
+    const uint32_t i = i0 + grp;
+    const bool have = i < nin;
+    uint2 it = make_uint2(0, 0);
+    Box<D> b;
+    uint64_t c0 = 0, c1 = 0;
+    if (have) {
+      it = in[i];
+      b = load_box<D>(boxes, it.x);
+      c0 = (uint64_t)it.y * fanout;
+      c1 = (c0 + fanout < nchild) ? c0 + fanout : nchild;
+    }
+    for (uint32_t r = 0; r < rounds; ++r) {
+      const uint64_t c = c0 + (uint64_t)r * LPI + gl;
       bool ov = false, in_ = false;
-      if (c < c1) test_node<D>(b, child_mbr, child_pad, c, ov, in_);
-      const uint32_t m = __ballot_sync(0xffffffffu, ov);
-      if (!m) continue;
+      if (have && c < c1) test_node<D>(b, child_mbr, child_pad, c, ov, in_);
+      const uint32_t wm = __ballot_sync(0xffffffffu, ov);
+      if (!wm) continue;  // warp-uniform
+      const uint32_t m = (wm >> (grp * LPI)) & kGroupMask;
       uint32_t base = 0;
-      if (lane == 0) base = atomicAdd(out_count, (uint32_t)__popc(m));
-      base = __shfl_sync(0xffffffffu, base, 0);
+      if (gl == 0 && m) base = atomicAdd(out_count, (uint32_t)__popc(m));
+      base = __shfl_sync(0xffffffffu, base, grp * LPI);
       if (ov) {
-        const uint64_t pos = (uint64_t)base + __popc(m & lane_lt_mask());
+        const uint64_t pos = (uint64_t)base + __popc(m & ((1u << gl) - 1u));
         if (pos < out_cap) {
           out[pos] = make_uint2(it.x, (uint32_t)c);
         } else {
           atomicOr(overflow, 1u);
         }
       }
-      if (lane == 0 && (uint64_t)base + __popc(m) > out_cap) atomicMax(need, base + __popc(m));
+      if (gl == 0 && m && (uint64_t)base + __popc(m) > out_cap) atomicMax(need, base + __popc(m));
     }
   }
 }
@@ -200,8 +216,19 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
           if (e1 > t.n) e1 = t.n;
           const int32_t* src = t.ids + e0;
           const uint64_t cnt = e1 - e0;
-          // four loads in flight per lane before their stores
+          // eight loads in flight per lane before their stores
           uint64_t j = lane;
+          for (; j + 224 < cnt; j += 256) {
+            int32_t v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = __ldg(src + j + 32 * k);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) out[wpos + j + 32 * k] = v[k];
+            if (hist) {
+#pragma unroll
+              for (int k = 0; k < 8; ++k) atomicAdd(wc + ((uint32_t)v[k] >> hist_bits), 1u);
+            }
+          }
           for (; j + 96 < cnt; j += 128) {
             const int32_t a = __ldg(src + j), b = __ldg(src + j + 32);
             const int32_t c = __ldg(src + j + 64), d = __ldg(src + j + 96);
@@ -500,9 +527,16 @@ template <int D>
 void launch_expand(uint32_t grid, cudaStream_t s, const float* boxes, const uint2* in,
                    const uint32_t* in_count, uint2* out, uint32_t* out_count, uint64_t cap,
                    const float* child_mbr, uint64_t nchild, uint64_t child_pad, uint32_t fanout,
-                   uint32_t* overflow, uint32_t* need) {
-  k_expand<D><<<grid, 256, 0, s>>>(boxes, in, in_count, out, out_count, cap, child_mbr, nchild,
-                                   child_pad, fanout, overflow, need);
+                   uint32_t* overflow, uint32_t* need, uint32_t lanes = 32) {
+  if (lanes == 8)
+    k_expand<D, 8><<<grid, 256, 0, s>>>(boxes, in, in_count, out, out_count, cap, child_mbr, nchild, child_pad,
+                                        fanout, overflow, need);
+  else if (lanes == 16)
+    k_expand<D, 16><<<grid, 256, 0, s>>>(boxes, in, in_count, out, out_count, cap, child_mbr, nchild, child_pad,
+                                         fanout, overflow, need);
+  else
+    k_expand<D, 32><<<grid, 256, 0, s>>>(boxes, in, in_count, out, out_count, cap, child_mbr, nchild, child_pad,
+                                         fanout, overflow, need);
 }
 
 // Ring buffers per warp that fit the leaf prefetch of this launch: at most
@@ -592,7 +626,7 @@ qcp_status expand_level(qcp_index* ix, Workspace* ws, uint32_t l, int cur, cudaS
   QCP_DISPATCH_D(ix->dims, launch_expand<DD>(grid, s, ws->boxes, ws->items[cur], ctr + kCtrFrontier0 + cur,
                                              ws->items[nxt], ctr + kCtrFrontier0 + nxt, ws->items_cap,
                                              t.mbr[l - 1], t.nodes[l - 1], t.pad[l - 1], t.fanout,
-                                             ctr + kCtrOverflow, ctr + kCtrNeedItems));
+                                             ctr + kCtrOverflow, ctr + kCtrNeedItems, ws->lanes_per_item));
   note_launch();
   return check_launch("k_expand");
 }

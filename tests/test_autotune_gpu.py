@@ -23,13 +23,26 @@ def data(workloads, oracle):
     return objs, boxes, want_offs, want_ids
 
 
-@pytest.mark.parametrize("bps,wb,lp", [(4, 16, 1), (16, 17, 2), (32, 12, 3), (1, 18, 4), (8, 17, 1), (8, 16, 3)])
-def test_knobs_keep_hits_exact(qcp, data, bps, wb, lp):
+@pytest.mark.parametrize("bps,wb,lp,lpi", [(4, 16, 1, 32), (16, 17, 2, 16), (32, 12, 3, 8), (1, 18, 4, 16),
+                                          (8, 17, 1, 8), (8, 16, 3, 32)])
+def test_knobs_keep_hits_exact(qcp, data, bps, wb, lp, lpi):
     objs, boxes, want_offs, want_ids = data
     with qcp.Index.build(objs, fanout=64) as ix:
-        res = ix.search(boxes, blocks_per_sm=bps, win_bits=wb, leaf_prefetch=lp)
+        res = ix.search(boxes, blocks_per_sm=bps, win_bits=wb, leaf_prefetch=lp, lanes_per_item=lpi)
         assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
-        assert np.array_equal(ix.counts(boxes, leaf_prefetch=lp), np.diff(want_offs))
+        assert np.array_equal(ix.counts(boxes, leaf_prefetch=lp, lanes_per_item=lpi), np.diff(want_offs))
+
+
+@pytest.mark.parametrize("lpi", [8, 16, 32])
+@pytest.mark.parametrize("fanout", [32, 96, 256])
+def test_lanes_per_item_at_every_fanout(qcp, data, lpi, fanout):
+    """Two or four (query, node) items per warp in the level expansion, at
+    fan-outs that are and are not multiples of the group width."""
+    objs, boxes, want_offs, want_ids = data
+    with qcp.Index.build(objs, fanout=fanout) as ix:
+        res = ix.search(boxes[:200], lanes_per_item=lpi)
+        n = int(want_offs[200])
+        assert_same_hits(res.offsets, res.ids, want_offs[:201], want_ids[:n])
 
 
 @pytest.mark.parametrize("fanout", [32, 128, 256])
@@ -74,12 +87,14 @@ def test_autotune_choice_and_trials(qcp, data):
     assert r["blocks_per_sm"] in (4, 8, 16)
     assert r["win_bits"] in (16, 17, 18)
     assert r["leaf_prefetch"] in (1, 2, 3)
-    assert len(r["trials"]) == 9  # 3 fan-outs, 2 more grids, 2 more windows, 2 more leaf tiles
+    assert r["lanes_per_item"] in (8, 16, 32)
+    # 3 fan-outs, 2 more grids, 2 more windows, 2 more leaf tiles, 2 more lane widths
+    assert len(r["trials"]) == 11
     assert r["best_ms"] == pytest.approx(min(t["ms"] for t in r["trials"]))
     chosen = [t for t in r["trials"] if t["ms"] == r["best_ms"]][0]
-    assert (chosen["fanout"], chosen["blocks_per_sm"], chosen["win_bits"], chosen["leaf_prefetch"]) == \
-        (r["fanout"], r["blocks_per_sm"], r["win_bits"], r["leaf_prefetch"])
+    keys = ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch", "lanes_per_item")
+    assert tuple(chosen[k] for k in keys) == tuple(r[k] for k in keys)
     with qcp.Index.build(objs, fanout=r["fanout"]) as ix:
         res = ix.search(boxes, blocks_per_sm=r["blocks_per_sm"], win_bits=r["win_bits"],
-                        leaf_prefetch=r["leaf_prefetch"])
+                        leaf_prefetch=r["leaf_prefetch"], lanes_per_item=r["lanes_per_item"])
         assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
