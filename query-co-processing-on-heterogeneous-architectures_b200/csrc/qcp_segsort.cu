@@ -589,21 +589,33 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     uint32_t pos = __reduce_add_sync(0xffffffffu, lane < wp ? ws : 0u) + ex;
     // one iteration per set bit (a flat loop: a warp runs as many iterations
     // as its lane with the most bits); the next nonzero word is fetched, and
-    // cleared, when the current one is used up
+    // cleared, when the current one is used up.  Ranks below kStage go to the
+    // stage and the rest straight to the output, in two loops so that no
+    // iteration tests the rank.
     uint32_t cur = 0, base = 0;
-    for (uint32_t left = cnt; left != 0; --left) {
+    const uint32_t nst = pos < kStage ? min(cnt, kStage - pos) : 0u;
+    int32_t* st = s.stage + pos;
+    for (uint32_t k = 0; k < nst; ++k) {
       if (cur == 0) {
         const uint32_t wi = __ffs(nz) - 1;
         nz &= nz - 1;
         cur = s.bm[tw0 + wi];
         s.bm[tw0 + wi] = 0u;
-        base = lo + ((tw0 + wi) << 5);
+        base = lo + ((tw0 + wi) << 5) - 1;
       }
-      const int32_t id = (int32_t)(base + __ffs(cur) - 1);
+      st[k] = (int32_t)(base + __ffs(cur));
       cur &= cur - 1;
-      if (pos < kStage) s.stage[pos] = id;
-      else dst[pos] = id;
-      ++pos;
+    }
+    for (uint32_t k = nst; k < cnt; ++k) {
+      if (cur == 0) {
+        const uint32_t wi = __ffs(nz) - 1;
+        nz &= nz - 1;
+        cur = s.bm[tw0 + wi];
+        s.bm[tw0 + wi] = 0u;
+        base = lo + ((tw0 + wi) << 5) - 1;
+      }
+      dst[pos + k] = (int32_t)(base + __ffs(cur));
+      cur &= cur - 1;
     }
     __syncthreads();
     // 3. staged ranks out
