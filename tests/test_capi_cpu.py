@@ -112,3 +112,25 @@ def test_newer_entry_points_reject_bad_arguments_without_device(qcp, tmp_path):
     assert lib.qcp_query_counts(None, buf, 2, None, counts) == BAD_ARG
     assert lib.qcp_index_load(str(tmp_path / "none.qcpidx").encode(), None, ctypes.byref(h)) == IO
     assert not h.value
+
+
+def test_build_plan_rejects_bad_arguments_without_device(qcp):
+    """The captured build checks its shape and key mode before touching a
+    device: n, dims, fan-out and key mode out of range are BAD_ARG."""
+    lib = qcp.load_library()
+    P = ctypes.c_void_p
+    h = P()
+    BAD_ARG = 1
+    assert lib.qcp_build_plan_create(0, 3, 0, None, ctypes.byref(h)) == BAD_ARG
+    assert lib.qcp_build_plan_create(1000, 9, 0, None, ctypes.byref(h)) == BAD_ARG
+    bo = qcp.BuildOpts(100, 0, 0, 0, None, 0, 0)  # fan-out not a multiple of 32
+    assert lib.qcp_build_plan_create(1000, 3, 0, ctypes.byref(bo), ctypes.byref(h)) == BAD_ARG
+    bo = qcp.BuildOpts(128, qcp.KEY_KMEANS, 0, 0, None, 0, 0)
+    assert lib.qcp_build_plan_create(1000, 3, 0, ctypes.byref(bo), ctypes.byref(h)) == BAD_ARG
+    assert b"k-means" in lib.qcp_last_error()
+    assert lib.qcp_build_plan_create(1000, 3, 0, None, None) == BAD_ARG
+    assert not h.value
+    assert lib.qcp_build_plan_run(None, None, 0, None, ctypes.byref(h)) == BAD_ARG
+    assert lib.qcp_build_plan_input(None) is None
+    assert lib.qcp_build_plan_free(None) == 0
+
