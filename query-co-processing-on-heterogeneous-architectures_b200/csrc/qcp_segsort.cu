@@ -81,9 +81,9 @@ struct BucketSmem {
 };
 
 // Slices of at most kTinyCap ids, one warp each (no CTA barriers): the ids
-// are counted into kTinyBuckets buckets by their top bits, a warp scan gives
-// the bucket bases, every id (read again, from L2) takes the next slot of its
-// bucket, each lane insertion-sorts its 8 buckets (a few ids each) and the
+// are loaded into registers (32 per lane, all loads in flight together) and
+// counted into kTinyBuckets buckets by their top bits, a warp scan gives the
+// bucket bases, every id takes the next slot of its bucket, each lane insertion-sorts its 8 buckets (a few ids each) and the
 // slice leaves in coalesced stores.  Jobs of more ids are k_sort_small's.
 struct TinySmem {
   uint32_t stage[kTinyWarps][kTinyCap];
@@ -91,7 +91,7 @@ struct TinySmem {
   uint32_t base[kTinyWarps][kTinyBuckets];
 };
 
-__global__ void __launch_bounds__(kTinyWarps * 32) k_sort_tiny(const Job* __restrict__ jobs,
+__global__ void __launch_bounds__(kTinyWarps * 32, 3) k_sort_tiny(const Job* __restrict__ jobs,
                                                                const uint32_t* __restrict__ njobs_p,
                                                                int32_t* out, uint32_t idbits) {
   const uint32_t njobs = *njobs_p;
@@ -112,8 +112,17 @@ __global__ void __launch_bounds__(kTinyWarps * 32) k_sort_tiny(const Job* __rest
     const uint32_t size = jb.size;
     if (size > kTinyCap) continue;  // warp-uniform
     const int32_t* src = out + jb.off;
-    // 1. bucket counts
-    for (uint32_t i = lane; i < size; i += 32) atomicAdd(&cnt[(uint32_t)__ldg(src + i) >> bshift], 1u);
+    // 1. the slice into registers (all loads in flight at once), bucket counts
+    constexpr uint32_t kPerLane = kTinyCap / 32;
+    uint32_t v[kPerLane];
+#pragma unroll
+    for (uint32_t k = 0; k < kPerLane; ++k) {
+      const uint32_t i = lane + 32 * k;
+      v[k] = (i < size) ? (uint32_t)__ldg(src + i) : kNone;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < kPerLane; ++k)
+      if (v[k] != kNone) atomicAdd(&cnt[v[k] >> bshift], 1u);
     __syncwarp();
     // 2. bucket bases: each lane owns kPer consecutive buckets
     uint32_t c[kPer];
@@ -133,10 +142,9 @@ __global__ void __launch_bounds__(kTinyWarps * 32) k_sort_tiny(const Job* __rest
     __syncwarp();
     // 3. every id to the next slot of its bucket (order inside a bucket is
     //    settled below)
-    for (uint32_t i = lane; i < size; i += 32) {
-      const uint32_t v = (uint32_t)__ldg(src + i);
-      stage[atomicAdd(&base[v >> bshift], 1u)] = v;
-    }
+#pragma unroll
+    for (uint32_t k = 0; k < kPerLane; ++k)
+      if (v[k] != kNone) stage[atomicAdd(&base[v[k] >> bshift], 1u)] = v[k];
     __syncwarp();
     // 4. insertion sort of each bucket [base - count, base); counts cleared
 #pragma unroll
