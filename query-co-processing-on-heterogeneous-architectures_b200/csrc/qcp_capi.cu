@@ -290,6 +290,27 @@ qcp_status ws_reserve_sort(qcp_index* ix, Workspace* ws, size_t jobs, size_t til
   return QCP_OK;
 }
 
+// The count pass's hit cache: group records for `items` items and
+// `mask_words` words of partial-leaf hit masks (each grown on its own).
+qcp_status ws_reserve_hitcache(Workspace* ws, size_t items, size_t mask_words) {
+  if (items && (!ws->item_grp || ws->item_grp_cap < items)) {
+    cudaFree(ws->item_grp);
+    ws->item_grp = nullptr;
+    ws->item_grp_cap = 0;
+    QCP_CUDA(cudaMalloc(&ws->item_grp, sizeof(uint32_t) * kMaxGroups * kGrpWords * items));
+    ws->item_grp_cap = items;
+  }
+  if (mask_words && (!ws->hmask || ws->hmask_cap < mask_words)) {
+    cudaFree(ws->hmask);
+    ws->hmask = nullptr;
+    ws->hmask_cap = 0;
+    const size_t n = mask_words + (mask_words >> 2) + 4096;
+    QCP_CUDA(cudaMalloc(&ws->hmask, sizeof(uint32_t) * n));
+    ws->hmask_cap = n;
+  }
+  return QCP_OK;
+}
+
 qcp_status ws_reserve_qwhist(Workspace* ws, size_t n) {
   size_t cap = ws->qwhist_cap;
   QCP_TRY(grow(&ws->qwhist, &cap, n, 4096));
@@ -304,6 +325,8 @@ void ws_destroy(Workspace* ws, qcp_index* ix) {
   cudaFree(ws->items[0]);
   cudaFree(ws->items[1]);
   cudaFree(ws->item_hits);
+  cudaFree(ws->item_grp);
+  cudaFree(ws->hmask);
   cudaFree(ws->qcount);
   cudaFree(ws->qcursor);
   if (ws->offsets) ix->pool.put(0, ws->offsets);

@@ -116,6 +116,14 @@ struct Workspace {
   uint32_t blocks_per_sm = 8;    // traversal grid = SMs x this, this call
   uint32_t win_bits = 18;        // sort window, this call
   uint32_t leaf_ring = 2;        // leaf prefetch buffers per warp, this call (< 2: none)
+  // hit cache of the count pass for the write pass: per item and 32-leaf
+  // group {overlap mask, covered mask, word offset of the group's partial
+  // leaves' hit masks in hmask}; per partially covered leaf its hit bits
+  uint32_t* item_grp = nullptr;
+  size_t item_grp_cap = 0;       // items
+  uint32_t* hmask = nullptr;
+  size_t hmask_cap = 0;          // words
+  bool use_hit_cache = false;    // this call's count pass fills the cache
   uint32_t lanes_per_item = 32;  // lanes of k_expand per (query, node) item, this call
   // CPU + GPU co-processing (QCP_ALGO_HYBRID) of this call
   bool hybrid = false;
@@ -154,6 +162,7 @@ enum CtrSlot : uint32_t {
   kCtrSmall = 7,      // small-segment job count
   kCtrWork2 = 8,
   kCtrTimeout = 9,    // nonzero: a bounded device wait ran out (results invalid)
+  kCtrMaskWords = 10, // hit-cache words the count pass asked for (may exceed the capacity)
   kCtrCount = 16
 };
 
@@ -378,6 +387,11 @@ constexpr uint32_t kHistMaxG = 256;
 // Default log2 of the per-query sort's id windows (qcp_query_opts.win_bits).
 constexpr uint32_t kDefaultWinBits = 17;
 qcp_status ws_reserve_qwhist(Workspace* ws, size_t n);
+// Words per (item, group) record of the hit cache and groups per item.
+constexpr uint32_t kGrpWords = 3;
+constexpr uint32_t kMaxGroups = 8;                    // fan-out <= 256
+constexpr uint32_t kNoMask = 0xffffffffu;            // group without cached hit masks
+qcp_status ws_reserve_hitcache(Workspace* ws, size_t items, size_t mask_words);
 // Workspace construction and buffer reservation (qcp_capi.cu).
 qcp_status ws_reserve_queries(qcp_index* ix, Workspace* ws, uint32_t q);
 qcp_status ws_reserve_items(qcp_index* ix, Workspace* ws, size_t items);

@@ -114,6 +114,23 @@ __host__ __device__ inline uint32_t ring_warp_bytes(uint32_t runs, uint32_t F, u
   return kRingHeader + nbuf * runs * F * 4u;
 }
 
+// Hit cache handed from the count pass to the write pass of one call.  The
+// count pass records, per item and 32-leaf group, the overlap and covered
+// masks of the group's leaves and where the hit bits of its partially
+// covered leaves start; per partially covered leaf and 128-object chunk it
+// records four words, bit l of word k = object 4l + k is a hit.  The write
+// pass then copies ids without testing a leaf MBR or a coordinate again.
+// grp == nullptr: no cache.  A group whose hit bits did not fit (mask words
+// past mask_cap) is marked kNoMask and the write pass tests its leaves.
+struct HitCache {
+  uint32_t* grp;       // [item][kMaxGroups][kGrpWords]
+  uint32_t* mask;      // hit bits
+  uint32_t mask_cap;   // words
+  uint32_t* cursor;    // words asked for so far (may pass mask_cap)
+};
+
+__device__ __forceinline__ uint32_t words_per_leaf(uint32_t F) { return ((F + 127u) / 128u) * 4u; }
+
 // Warp per (query, level-1 node) item.  COUNT: item_hits[i] and qcount[q].
 // WRITE: ids at out[offsets[q] + reserved slice].
 // PF: the partially covered leaves of an item are fetched into the warp's
@@ -131,7 +148,8 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
                                                   unsigned long long* qcursor,
                                                   int32_t* __restrict__ out, uint64_t item_cap,
                                                   unsigned long long* stats, uint32_t* qwhist, uint32_t hist_G,
-                                                  uint32_t hist_bits, uint32_t nbuf, uint32_t* err) {
+                                                  uint32_t hist_bits, uint32_t nbuf, uint32_t* err,
+                                                  HitCache hc) {
   // write pass of the sorted path: per-(query, window) id counts in per-warp
   // shared counters, flushed once per item
   __shared__ uint32_t wcount[8][MODE == kWrite ? kHistMaxG : 1];
@@ -185,12 +203,42 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
     uint32_t npart = 0;  // PF: partially covered leaves listed for the ring
     const uint64_t l0 = (uint64_t)it.y * F;
     const uint64_t l1 = (l0 + F < nleaves) ? l0 + F : nleaves;
+    const bool cache = hc.grp != nullptr;
+    const uint32_t wpl = words_per_leaf(F);
+    uint32_t* grec = cache ? hc.grp + (size_t)i * (kMaxGroups * kGrpWords) : nullptr;
     for (uint64_t lb = l0; lb < l1; lb += 32) {
+      const uint32_t gi = (uint32_t)((lb - l0) >> 5);
       const uint64_t leaf = lb + lane;
       bool ov = false, in_ = false;
-      if (leaf < l1) test_node<D>(b, lmbr, lpad, leaf, ov, in_);
-      const uint32_t mov = __ballot_sync(0xffffffffu, ov);
-      const uint32_t min_ = __ballot_sync(0xffffffffu, in_ && ov);
+      uint32_t mov, min_, moff = kNoMask;
+      if (MODE == kWrite && cache) {
+        // the count pass's masks of this group
+        mov = grec[gi * kGrpWords + 0];
+        min_ = grec[gi * kGrpWords + 1];
+        moff = grec[gi * kGrpWords + 2];
+      } else {
+        if (leaf < l1) test_node<D>(b, lmbr, lpad, leaf, ov, in_);
+        mov = __ballot_sync(0xffffffffu, ov);
+        min_ = __ballot_sync(0xffffffffu, in_ && ov);
+        if (MODE == kCount && cache) {
+          // record the group; room for its partial leaves' hit bits (the
+          // ring path reserves for the whole item below)
+          const uint32_t np = __popc(mov & ~min_);
+          if (!PF && np) {
+            if (lane == 0) {
+              const uint32_t want = np * wpl;
+              moff = atomicAdd(hc.cursor, want);
+              if ((uint64_t)moff + want > hc.mask_cap) moff = kNoMask;
+            }
+            moff = __shfl_sync(0xffffffffu, moff, 0);
+          }
+          if (lane == 0) {
+            grec[gi * kGrpWords + 0] = mov;
+            grec[gi * kGrpWords + 1] = min_;
+            grec[gi * kGrpWords + 2] = moff;
+          }
+        }
+      }
       if (!mov) continue;
       // leaves whose MBR lies inside the query: every object is a hit
       if (MODE == kCount) {
@@ -252,23 +300,41 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
         }
       }
       uint32_t mp = mov & ~min_;
+      const bool replay = MODE == kWrite && moff != kNoMask;  // hit bits cached by the count pass
       if constexpr (PF) {
-        // listed for the prefetch ring below
-        if ((mp >> lane) & 1u) plist[npart + __popc(mp & lane_lt_mask())] = (uint8_t)(lb - l0 + lane);
-        npart += __popc(mp);
-        mp = 0;
+        if (!replay) {
+          // listed for the prefetch ring below
+          if ((mp >> lane) & 1u) plist[npart + __popc(mp & lane_lt_mask())] = (uint8_t)(lb - l0 + lane);
+          npart += __popc(mp);
+          mp = 0;
+        }
       }
-      // partially covered leaves: test every object
+      // partially covered leaves: test every object, or replay its hit bits
+      uint32_t jl = 0;  // index of the leaf among the group's partial leaves
       while (mp) {
         const int s = __ffs(mp) - 1;
         mp &= mp - 1;
         const uint64_t e0 = (lb + s) * F;
+        const uint32_t* mw = (moff != kNoMask) ? hc.mask + moff + jl * wpl : nullptr;
+        ++jl;
         for (uint32_t g0 = 0; g0 < F; g0 += 128) {  // warp-uniform trip count
           const uint32_t g = g0 + lane * 4;
           const uint64_t p = e0 + g;
-          const uint32_t hm = (g < F) ? test4<D, RECT>(b, t.coords, t.npad, p, t.n) : 0u;
+          uint32_t hm;
+          if (replay) {
+            const uint4 w = *reinterpret_cast<const uint4*>(mw + (g0 >> 5));
+            hm = ((w.x >> lane) & 1u) | (((w.y >> lane) & 1u) << 1) | (((w.z >> lane) & 1u) << 2) |
+                 (((w.w >> lane) & 1u) << 3);
+          } else {
+            hm = (g < F) ? test4<D, RECT>(b, t.coords, t.npad, p, t.n) : 0u;
+          }
           if (MODE == kCount) {
             hits += __popc(hm);
+            if (mw) {
+              const uint32_t b0 = __ballot_sync(0xffffffffu, hm & 1u), b1 = __ballot_sync(0xffffffffu, hm & 2u);
+              const uint32_t b2 = __ballot_sync(0xffffffffu, hm & 4u), b3 = __ballot_sync(0xffffffffu, hm & 8u);
+              if (lane == 0) *reinterpret_cast<uint4*>(const_cast<uint32_t*>(mw) + (g0 >> 5)) = make_uint4(b0, b1, b2, b3);
+            }
           } else {
             uint32_t tot;
             const uint32_t ex = warp_excl_sum(__popc(hm), &tot);
@@ -291,21 +357,41 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
         }
       }
     }
+    // ring path of the count pass with the cache: room for the hit bits of
+    // the item's listed leaves (list order = group order), recorded per group
+    uint32_t ring_moff = kNoMask;
+    if (PF && MODE == kCount && cache && npart) {
+      if (lane == 0) {
+        const uint32_t want = npart * wpl;
+        ring_moff = atomicAdd(hc.cursor, want);
+        if ((uint64_t)ring_moff + want > hc.mask_cap) ring_moff = kNoMask;
+        uint32_t before = 0;
+        for (uint32_t gi = 0; gi * 32 < (uint32_t)(l1 - l0); ++gi) {
+          const uint32_t np = __popc(grec[gi * kGrpWords + 0] & ~grec[gi * kGrpWords + 1]);
+          if (np && ring_moff != kNoMask) grec[gi * kGrpWords + 2] = ring_moff + before * wpl;
+          before += np;
+        }
+      }
+      ring_moff = __shfl_sync(0xffffffffu, ring_moff, 0);
+    }
     if (PF && npart) {
       // partially covered leaves through the ring: leaf k of the list goes
       // to buffer k % nbuf, nbuf leaves ahead of the one being tested
       __syncwarp();  // the list is complete
       const uint32_t run_bytes = F * 4u;
+      // one lane arms the buffer's barrier and issues the leaf's NR copies;
+      // the warp's reads of the buffer's previous leaf are done (they fed
+      // the tests before this point, and the syncwarp orders every lane's)
       auto issue = [&](uint32_t k, uint32_t bb) {
-        const uint64_t leaf = l0 + plist[k];
-        fence_proxy_async_smem();  // this buffer's earlier reads before the copy
         __syncwarp();
-        if (lane == 0) mbar_arrive_expect_tx(&bars[bb], NR * run_bytes);
-        __syncwarp();
-        if (lane < NR) {
-          const void* src = (lane < NC) ? (const void*)(t.coords + (uint64_t)lane * t.npad + leaf * F)
-                                        : (const void*)(t.ids + leaf * F);
-          bulk_copy_g2s(bufs + (size_t)bb * buf_floats + lane * F, src, run_bytes, &bars[bb]);
+        if (lane == 0) {
+          const uint64_t leaf = l0 + plist[k];
+          float* dst = bufs + (size_t)bb * buf_floats;
+          mbar_arrive_expect_tx(&bars[bb], NR * run_bytes);
+#pragma unroll
+          for (uint32_t r = 0; r < NC; ++r)
+            bulk_copy_g2s(dst + r * F, t.coords + (uint64_t)r * t.npad + leaf * F, run_bytes, &bars[bb]);
+          if (NR > NC) bulk_copy_g2s(dst + NC * F, t.ids + leaf * F, run_bytes, &bars[bb]);
         }
         pending |= 1u << bb;
       };
@@ -328,6 +414,12 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
           const uint32_t hm = (g < F) ? test4_staged<D, RECT>(b, sb, F, g, valid) : 0u;
           if (MODE == kCount) {
             hits += __popc(hm);
+            if (ring_moff != kNoMask) {
+              const uint32_t b0 = __ballot_sync(0xffffffffu, hm & 1u), b1 = __ballot_sync(0xffffffffu, hm & 2u);
+              const uint32_t b2 = __ballot_sync(0xffffffffu, hm & 4u), b3 = __ballot_sync(0xffffffffu, hm & 8u);
+              if (lane == 0)
+                *reinterpret_cast<uint4*>(hc.mask + ring_moff + k * wpl + (g0 >> 5)) = make_uint4(b0, b1, b2, b3);
+            }
           } else {
             uint32_t tot;
             const uint32_t ex = warp_excl_sum(__popc(hm), &tot);
@@ -554,7 +646,7 @@ void launch_leafscan_t(uint32_t grid, cudaStream_t s, const TreeView& t, const f
                        const uint32_t* item_count, uint32_t* work, uint32_t* item_hits, uint64_t* qcount,
                        const uint64_t* offsets, uint64_t* qcursor, int32_t* out, uint64_t item_cap,
                        unsigned long long* stats, uint32_t* qwhist, uint32_t hist_G, uint32_t hist_bits,
-                       uint32_t ring, uint32_t* err) {
+                       uint32_t ring, uint32_t* err, HitCache hc) {
   const uint32_t nb = ring_buffers(leaf_runs(D, RECT, MODE), t.fanout, ring);
   if (nb) {
     const size_t smem = 8u * (size_t)ring_warp_bytes(leaf_runs(D, RECT, MODE), t.fanout, nb);
@@ -568,12 +660,12 @@ void launch_leafscan_t(uint32_t grid, cudaStream_t s, const TreeView& t, const f
     if (fit >= 1 && grid > sms * fit) grid = sms * fit;
     kern<<<grid, 256, smem, s>>>(t, boxes, items, item_count, work, item_hits, (unsigned long long*)qcount,
                                  (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap,
-                                 stats, qwhist, hist_G, hist_bits, nb, err);
+                                 stats, qwhist, hist_G, hist_bits, nb, err, hc);
   } else {
     k_leafscan<D, RECT, MODE, false><<<grid, 256, 0, s>>>(
         t, boxes, items, item_count, work, item_hits, (unsigned long long*)qcount,
         (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap, stats, qwhist, hist_G,
-        hist_bits, 0u, err);
+        hist_bits, 0u, err, hc);
   }
 }
 
@@ -583,13 +675,13 @@ void launch_leafscan(bool rect, uint32_t grid, cudaStream_t s, const TreeView& t
                      uint32_t* item_hits, uint64_t* qcount, const uint64_t* offsets,
                      uint64_t* qcursor, int32_t* out, uint64_t item_cap,
                      unsigned long long* stats, uint32_t* qwhist, uint32_t hist_G,
-                     uint32_t hist_bits, uint32_t ring, uint32_t* err) {
+                     uint32_t hist_bits, uint32_t ring, uint32_t* err, HitCache hc = HitCache{}) {
   if (rect)
     launch_leafscan_t<D, true, MODE>(grid, s, t, boxes, items, item_count, work, item_hits, qcount, offsets, qcursor,
-                                     out, item_cap, stats, qwhist, hist_G, hist_bits, ring, err);
+                                     out, item_cap, stats, qwhist, hist_G, hist_bits, ring, err, hc);
   else
     launch_leafscan_t<D, false, MODE>(grid, s, t, boxes, items, item_count, work, item_hits, qcount, offsets,
-                                      qcursor, out, item_cap, stats, qwhist, hist_G, hist_bits, ring, err);
+                                      qcursor, out, item_cap, stats, qwhist, hist_G, hist_bits, ring, err, hc);
 }
 
 template <int D, int MODE>
@@ -631,6 +723,13 @@ qcp_status expand_level(qcp_index* ix, Workspace* ws, uint32_t l, int cur, cudaS
   return check_launch("k_expand");
 }
 
+// The hit cache of this call (ws->use_hit_cache), or none.
+static HitCache hit_cache_of(Workspace* ws) {
+  if (!ws->use_hit_cache || !ws->item_grp || !ws->hmask) return HitCache{nullptr, nullptr, 0, nullptr};
+  return HitCache{ws->item_grp, ws->hmask, (uint32_t)(ws->hmask_cap > 0xfffffff0u ? 0xfffffff0u : ws->hmask_cap),
+                  ws->ctr + kCtrMaskWords};
+}
+
 qcp_status write_items(qcp_index* ix, Workspace* ws, int cur, cudaStream_t s) {
   const TreeView t = view_of(ix);
   const uint32_t grid = (uint32_t)num_sms() * ws->blocks_per_sm;
@@ -640,7 +739,8 @@ qcp_status write_items(qcp_index* ix, Workspace* ws, int cur, cudaStream_t s) {
                                                        ws->item_hits, nullptr, ws->offsets, ws->qcursor,
                                                        ws->out_ids, ws->items_cap, ws->d_stats,
                                                        ws->hist_G ? ws->qwhist : nullptr, ws->hist_G,
-                                                       ws->hist_bits, ws->leaf_ring, ctr + kCtrTimeout));
+                                                       ws->hist_bits, ws->leaf_ring, ctr + kCtrTimeout,
+                                                       hit_cache_of(ws)));
   note_launch();
   return check_launch("k_leafscan<write>");
 }
@@ -655,6 +755,7 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
   uint32_t* ctr = ws->ctr;
   // start level: items at level `start` are (query, node) pairs
   const uint32_t start = (ix->levels >= 2) ? ix->levels - 1 : 1;
+  ws->use_hit_cache = false;
   for (int attempt = 0; attempt < 8; ++attempt) {
     mark(ws, kEvStart, s);
     QCP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * kCtrCount, s));
@@ -685,11 +786,14 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
     mark(ws, kEvExpand, s);
     // the level-1 items must fit the per-item hit array too
     QCP_TRY(ws_reserve_items(ix, ws, 0));
+    // a call that writes ids keeps the count pass's hits for the write pass
+    ws->use_hit_cache = !counts_only;
+    if (ws->use_hit_cache) QCP_TRY(ws_reserve_hitcache(ws, ws->items_cap, ws->hmask_cap ? 0 : (size_t)1 << 20));
     QCP_DISPATCH_D(D, launch_leafscan<DD, kCount>(rect, grid, s, t, ws->boxes, ws->items[cur],
                                                   ctr + kCtrFrontier0 + cur, ctr + kCtrWork,
                                                   ws->item_hits, ws->qcount, nullptr, nullptr, nullptr,
                                                   ws->items_cap, ws->d_stats, nullptr, 0, 0, ws->leaf_ring,
-                                                  ctr + kCtrTimeout));
+                                                  ctr + kCtrTimeout, hit_cache_of(ws)));
     note_launch();
     QCP_TRY(check_launch("k_leafscan<count>"));
     mark(ws, kEvCount, s);
@@ -740,6 +844,13 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
         }
       }
     }
+    // hit bits that did not fit this call were tested again by the write
+    // pass; the next call gets room for them (after this call's passes)
+    if (ws->use_hit_cache && ws->h_ctr[kCtrMaskWords] > ws->hmask_cap) {
+      QCP_CUDA(cudaStreamSynchronize(s));
+      QCP_TRY(ws_reserve_hitcache(ws, 0, ws->h_ctr[kCtrMaskWords]));
+    }
+    ws->use_hit_cache = false;
     return QCP_OK;
   }
   set_error("query frontier did not fit after repeated growth");
@@ -840,6 +951,7 @@ qcp_status run_batched_device(qcp_index* ix, Workspace* ws, uint32_t q, uint64_t
   const uint32_t grid = (uint32_t)num_sms() * ws->blocks_per_sm;
   uint32_t* ctr = ws->ctr;
   const uint32_t start = (ix->levels >= 2) ? ix->levels - 1 : 1;
+  ws->use_hit_cache = false;  // the captured pipeline tests every leaf in both passes
   QCP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * kCtrCount, s));
   QCP_CUDA(cudaMemsetAsync(ws->qcount, 0, sizeof(uint64_t) * q, s));
   QCP_TRY(init_items(ws, q, s));

@@ -168,7 +168,8 @@ __global__ void __launch_bounds__(kTinyWarps * 32, 3) k_sort_tiny(const Job* __r
   }
 }
 
-__global__ void __launch_bounds__(kSmallThreads) k_sort_small(const Job* __restrict__ jobs,
+// jobs_end: one past the last job; job j is jobs_end[-1 - j].
+__global__ void __launch_bounds__(kSmallThreads) k_sort_small(const Job* __restrict__ jobs_end,
                                                               const uint32_t* __restrict__ njobs_p,
                                                               int32_t* out, uint32_t idbits) {
   const uint32_t njobs = *njobs_p;
@@ -180,9 +181,8 @@ __global__ void __launch_bounds__(kSmallThreads) k_sort_small(const Job* __restr
   for (uint32_t i = tid; i < kBuckets; i += kSmallThreads) s.cnt[i] = 0;
   __syncthreads();
   for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
-    const Job jb = jobs[j];
+    const Job jb = jobs_end[-1 - (long long)j];
     const uint32_t size = jb.size;
-    if (size <= kTinyCap) continue;  // CTA-uniform: k_sort_tiny's job
     // 1. count into buckets; each id's slot in its bucket is kept by index
     for (uint32_t i0 = 0; i0 < size; i0 += kSmallThreads * 8) {
       uint32_t v[8];
@@ -262,8 +262,13 @@ __global__ void __launch_bounds__(kSmallThreads) k_sort_small(const Job* __restr
 // ============================================================================
 // Window partition
 // ============================================================================
+// Job lists by slice size: slices of <= kTinyCap ids from the front of
+// `small` (count *ntiny), slices of <= kSmallCap ids from its back (small[cap -
+// 1 - k], count *nsmall), larger ones in `big`.  Slices of 0 or 1 ids are
+// sorted already.
 __global__ void k_classify(const unsigned long long* __restrict__ offsets, uint32_t q, Job* small,
-                           uint32_t* nsmall, Job* big, uint32_t* nbig, unsigned long long* big_ids) {
+                           uint32_t* ntiny, uint32_t* nsmall, size_t cap, Job* big, uint32_t* nbig,
+                           unsigned long long* big_ids) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < q; i += gridDim.x * blockDim.x) {
     const unsigned long long off = offsets[i];
     const unsigned long long sz = offsets[i + 1] - off;
@@ -272,8 +277,10 @@ __global__ void k_classify(const unsigned long long* __restrict__ offsets, uint3
     j.off = off;
     j.size = (uint32_t)sz;
     j.q = i;
-    if (sz <= kSmallCap) {
-      small[atomicAdd(nsmall, 1u)] = j;
+    if (sz <= kTinyCap) {
+      small[atomicAdd(ntiny, 1u)] = j;
+    } else if (sz <= kSmallCap) {
+      small[cap - 1 - atomicAdd(nsmall, 1u)] = j;
     } else {
       big[atomicAdd(nbig, 1u)] = j;
       if (big_ids) atomicAdd(big_ids, sz);
@@ -710,25 +717,31 @@ qcp_status sort_small_slices(qcp_index* ix, Workspace* ws, uint32_t q, cudaStrea
   QCP_TRY(set_sort_attrs(ix, scatter_max));
   QCP_TRY(ws_reserve_sort(ix, ws, (size_t)q + 256, 0));
   uint32_t* ctr = ws->ctr;
-  QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t) * 2, s));
+  QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t) * 3, s));  // jobs0, jobs1, small
   Job* small = reinterpret_cast<Job*>(ws->jobs[0]);
   Job* big = reinterpret_cast<Job*>(ws->jobs[1]);
   k_classify<<<(q + 255) / 256, 256, 0, s>>>((const unsigned long long*)ws->offsets, q, small,
-                                             ctr + kCtrJobs0, big, ctr + kCtrJobs1,
+                                             ctr + kCtrJobs0, ctr + kCtrSmall, ws->jobs_cap, big, ctr + kCtrJobs1,
                                              ws->timing ? ws->d_stats + kStatWindowIds : nullptr);
   note_launch();
   QCP_CUDA(cudaMemcpyAsync(ws->h_ctr, ctr, sizeof(uint32_t) * kCtrCount, cudaMemcpyDeviceToHost, s));
   QCP_CUDA(cudaStreamSynchronize(s));
-  const uint32_t nsmall = ws->h_ctr[kCtrJobs0];
+  const uint32_t ntiny = ws->h_ctr[kCtrJobs0];
+  const uint32_t nsmall = ws->h_ctr[kCtrSmall];
   const uint32_t nbig = ws->h_ctr[kCtrJobs1];
-  ws->sort_small_jobs = nsmall;
+  ws->sort_small_jobs = ntiny + nsmall;
   ws->sort_msd_jobs = nbig;
-  if (nsmall) {
-    k_sort_tiny<<<min((nsmall + kTinyWarps - 1) / kTinyWarps, sms * 4), kTinyWarps * 32, sizeof(TinySmem), s>>>(
+  if (ntiny) {
+    k_sort_tiny<<<min((ntiny + kTinyWarps - 1) / kTinyWarps, sms * 4), kTinyWarps * 32, sizeof(TinySmem), s>>>(
         small, ctr + kCtrJobs0, ws->out_ids, idbits);
-    k_sort_small<<<min(nsmall, sms * 3), kSmallThreads, sizeof(BucketSmem), s>>>(small, ctr + kCtrJobs0,
-                                                                                  ws->out_ids, idbits);
-    note_launch(2);
+    note_launch();
+    QCP_TRY(check_launch("k_sort_tiny"));
+  }
+  if (nsmall) {
+    k_sort_small<<<min(nsmall, sms * 3), kSmallThreads, sizeof(BucketSmem), s>>>(small + ws->jobs_cap,
+                                                                                  ctr + kCtrSmall, ws->out_ids,
+                                                                                  idbits);
+    note_launch();
     QCP_TRY(check_launch("k_sort_small"));
   }
   *big_out = big;
@@ -862,11 +875,13 @@ qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void*
   unsigned long long* wcur = wbase + nw;
   uint32_t* tiles = reinterpret_cast<uint32_t*>(wcur + nw);
   uint32_t* tile_off = tiles + q;
-  QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t) * 2, s));
+  QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t) * 3, s));  // jobs0, jobs1, small
   k_classify<<<(q + 255) / 256, 256, 0, s>>>((const unsigned long long*)ws->offsets, q, small, ctr + kCtrJobs0,
+                                             ctr + kCtrSmall, ws->jobs_cap,
                                              big, ctr + kCtrJobs1, nullptr);
   k_sort_tiny<<<sms * 4, kTinyWarps * 32, sizeof(TinySmem), s>>>(small, ctr + kCtrJobs0, ws->out_ids, idbits);
-  k_sort_small<<<sms * 3, kSmallThreads, sizeof(BucketSmem), s>>>(small, ctr + kCtrJobs0, ws->out_ids, idbits);
+  k_sort_small<<<sms * 3, kSmallThreads, sizeof(BucketSmem), s>>>(small + ws->jobs_cap, ctr + kCtrSmall,
+                                                                  ws->out_ids, idbits);
   note_launch();
   k_tiles_per_job<<<(q + 255) / 256, 256, 0, s>>>(big, ctr + kCtrJobs1, q, tiles);
   note_launch(3);

@@ -223,3 +223,22 @@ def test_slice_sizes_at_every_sort_boundary(qcp, oracle):
         for algo in ["batched", "plain"]:
             res = ix.search(boxes, algo=algo)
             assert_same_hits(res.offsets, res.ids, want_offs, want_ids, boxes)
+
+
+def test_hit_cache_overflow_then_full(qcp, oracle, workloads):
+    """The write pass replays the count pass's leaf masks and hit bits.  The
+    first call on a fresh index has room for 2^20 words of hit bits; this
+    batch needs more (about 300,000 partially covered leaves), so part of its
+    groups are tested again by the write pass; the second call has room for
+    all.  Both must equal the oracle, sorted and unsorted."""
+    pts = workloads.uniform_points(2_000_000, 3, seed=23)
+    boxes = workloads.fixed_cubes(3000, 3, 0.16, seed=24)
+    want_offs, want_ids = oracle.ids(pts, 3, False, boxes, threads=16)
+    with qcp.Index.build(pts) as ix:
+        for _ in range(2):
+            res = ix.search(boxes)
+            assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
+        res = ix.search(boxes, sort=False)
+        assert np.array_equal(res.offsets, want_offs)
+        for i in range(0, len(boxes), 97):
+            assert np.array_equal(np.sort(res.hits(i)), want_ids[want_offs[i]:want_offs[i + 1]])
