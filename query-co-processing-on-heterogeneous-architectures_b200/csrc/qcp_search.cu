@@ -130,6 +130,7 @@ struct HitCache {
 };
 
 __device__ __forceinline__ uint32_t words_per_leaf(uint32_t F) { return ((F + 127u) / 128u) * 4u; }
+constexpr uint32_t kMaskChunk = 1024;  // hit-cache words a warp takes at a time
 
 // Warp per (query, level-1 node) item.  COUNT: item_hits[i] and qcount[q].
 // WRITE: ids at out[offsets[q] + reserved slice].
@@ -180,6 +181,28 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
     }
     __syncwarp();
   }
+  // hit-bit room in per-warp chunks of the global cursor (one atomic per
+  // chunk, not per group); kNoMask once the cache's capacity is used up
+  uint32_t ch_pos = 0, ch_end = 0;
+  bool ch_out = false;
+  auto mask_alloc = [&](uint32_t want) -> uint32_t {
+    if (ch_pos + want > ch_end) {
+      if (ch_out) return kNoMask;
+      const uint32_t grab = want > kMaskChunk ? want : kMaskChunk;
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(hc.cursor, grab);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if ((uint64_t)base + grab > hc.mask_cap) {
+        ch_out = true;
+        return kNoMask;
+      }
+      ch_pos = base;
+      ch_end = base + grab;
+    }
+    const uint32_t r = ch_pos;
+    ch_pos += want;
+    return r;
+  };
   const uint32_t nitems = (uint32_t)min((uint64_t)*item_count, item_cap);
   const float* lmbr = t.mbr[0];
   const uint64_t lpad = t.pad[0];
@@ -206,6 +229,7 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
     const bool cache = hc.grp != nullptr;
     const uint32_t wpl = words_per_leaf(F);
     uint32_t* grec = cache ? hc.grp + (size_t)i * (kMaxGroups * kGrpWords) : nullptr;
+    uint32_t g_mov = 0, g_min = 0;  // ring path: lane g holds group g's masks
     for (uint64_t lb = l0; lb < l1; lb += 32) {
       const uint32_t gi = (uint32_t)((lb - l0) >> 5);
       const uint64_t leaf = lb + lane;
@@ -221,21 +245,21 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
         mov = __ballot_sync(0xffffffffu, ov);
         min_ = __ballot_sync(0xffffffffu, in_ && ov);
         if (MODE == kCount && cache) {
-          // record the group; room for its partial leaves' hit bits (the
-          // ring path reserves for the whole item below)
-          const uint32_t np = __popc(mov & ~min_);
-          if (!PF && np) {
-            if (lane == 0) {
-              const uint32_t want = np * wpl;
-              moff = atomicAdd(hc.cursor, want);
-              if ((uint64_t)moff + want > hc.mask_cap) moff = kNoMask;
+          if (PF) {
+            // recorded after the loop, with room for the whole item
+            if (lane == gi) {
+              g_mov = mov;
+              g_min = min_;
             }
-            moff = __shfl_sync(0xffffffffu, moff, 0);
-          }
-          if (lane == 0) {
-            grec[gi * kGrpWords + 0] = mov;
-            grec[gi * kGrpWords + 1] = min_;
-            grec[gi * kGrpWords + 2] = moff;
+          } else {
+            // record the group with room for its partial leaves' hit bits
+            const uint32_t np = __popc(mov & ~min_);
+            if (np) moff = mask_alloc(np * wpl);
+            if (lane == 0) {
+              grec[gi * kGrpWords + 0] = mov;
+              grec[gi * kGrpWords + 1] = min_;
+              grec[gi * kGrpWords + 2] = moff;
+            }
           }
         }
       }
@@ -358,21 +382,20 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
       }
     }
     // ring path of the count pass with the cache: room for the hit bits of
-    // the item's listed leaves (list order = group order), recorded per group
+    // the item's listed leaves (list order = group order); lane g records
+    // group g
     uint32_t ring_moff = kNoMask;
-    if (PF && MODE == kCount && cache && npart) {
-      if (lane == 0) {
-        const uint32_t want = npart * wpl;
-        ring_moff = atomicAdd(hc.cursor, want);
-        if ((uint64_t)ring_moff + want > hc.mask_cap) ring_moff = kNoMask;
-        uint32_t before = 0;
-        for (uint32_t gi = 0; gi * 32 < (uint32_t)(l1 - l0); ++gi) {
-          const uint32_t np = __popc(grec[gi * kGrpWords + 0] & ~grec[gi * kGrpWords + 1]);
-          if (np && ring_moff != kNoMask) grec[gi * kGrpWords + 2] = ring_moff + before * wpl;
-          before += np;
-        }
+    if (PF && MODE == kCount && cache) {
+      const uint32_t ngroups = (uint32_t)((l1 - l0 + 31) >> 5);
+      const uint32_t np = lane < ngroups ? __popc(g_mov & ~g_min) : 0u;
+      uint32_t tot;
+      const uint32_t before = warp_excl_sum(np, &tot);
+      if (tot) ring_moff = mask_alloc(tot * wpl);
+      if (lane < ngroups) {
+        grec[lane * kGrpWords + 0] = g_mov;
+        grec[lane * kGrpWords + 1] = g_min;
+        grec[lane * kGrpWords + 2] = (np && ring_moff != kNoMask) ? ring_moff + before * wpl : kNoMask;
       }
-      ring_moff = __shfl_sync(0xffffffffu, ring_moff, 0);
     }
     if (PF && npart) {
       // partially covered leaves through the ring: leaf k of the list goes

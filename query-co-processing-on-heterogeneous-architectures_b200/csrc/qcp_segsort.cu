@@ -486,6 +486,12 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// Position of bitmap word w in shared memory (see k_win_sort).
+template <uint32_t BITS>
+__device__ __forceinline__ uint32_t bm_at(uint32_t w) {
+  return (w % kLaneWords) * WinCfg<BITS>::kThreads + w / kLaneWords;
+}
+
 // Persistent CTAs over the (job, window) pairs g = job * G + window.
 //   1. every id of window g (read from src, the scratch buffer) sets its bit
 //      in a bitmap of the window's 2^wbits possible ids; its first kPrefetch
@@ -518,10 +524,10 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
   const uint32_t nwords = (1u << wbits) >> 5;   // 12 <= wbits <= BITS
   const uint32_t tw0 = tid * kLaneWords;        // this thread's words [tw0, tw0 + kLaneWords)
   const bool owner = tw0 < nwords;
-  // the four 16-byte groups of a thread's words are read starting at group
-  // (tid >> 1) & 3, so that the 8 threads of a shared-memory phase hit 32
-  // distinct banks
-  const uint32_t rot = (tid >> 1) & 3;
+  // Word w of the bitmap (thread w / kLaneWords's word w % kLaneWords) is
+  // stored at bm_at(w) = (w % kLaneWords) * kRankThreads + w / kLaneWords, so
+  // that the lanes of a warp reading or clearing one word each of their own
+  // ranges always hit 32 distinct banks.
   for (uint32_t i = tid; i < kBmWords / 4; i += kRankThreads) bm4[i] = make_uint4(0, 0, 0, 0);
   __syncthreads();
   // the first kPrefetch ids of window g + gridDim.x are copied into s.pf
@@ -554,7 +560,7 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
       const uint32_t npf = size < kPrefetch ? size : kPrefetch;
       for (uint32_t i = tid; i < npf; i += kRankThreads) {
         const uint32_t x = (uint32_t)s.pf[i] - lo;
-        atomicOr(&s.bm[x >> 5], 1u << (x & 31));
+        atomicOr(&s.bm[bm_at<BITS>(x >> 5)], 1u << (x & 31));
       }
       for (uint32_t i0 = kPrefetch; i0 < size; i0 += kBatch * kRankThreads) {
         uint32_t a[kBatch];
@@ -567,7 +573,7 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
 #pragma unroll
         for (uint32_t k = 0; k < kBatch; ++k)
           if (i0 + k * kRankThreads + (wp << 5) < size && a[k] != kNone)
-            atomicOr(&s.bm[a[k] >> 5], 1u << (a[k] & 31));
+            atomicOr(&s.bm[bm_at<BITS>(a[k] >> 5)], 1u << (a[k] & 31));
       }
     } else if (size == 1 && tid == 0) {
       dst[0] = s.pf[0];
@@ -587,12 +593,10 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     uint32_t cnt = 0, nz = 0;
     if (owner) {
 #pragma unroll
-      for (uint32_t k = 0; k < 4; ++k) {
-        const uint32_t gi = (k + rot) & 3;
-        const uint4 v = bm4[(tw0 >> 2) + gi];
-        cnt += __popc(v.x) + __popc(v.y) + __popc(v.z) + __popc(v.w);
-        const uint32_t m = (v.x ? 1u : 0u) | (v.y ? 2u : 0u) | (v.z ? 4u : 0u) | (v.w ? 8u : 0u);
-        nz |= m << (gi * 4);
+      for (uint32_t k = 0; k < kLaneWords; ++k) {
+        const uint32_t v = s.bm[k * kRankThreads + tid];
+        cnt += __popc(v);
+        nz |= (v ? 1u : 0u) << k;
       }
     }
     uint32_t wtot;
@@ -614,8 +618,8 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
       if (cur == 0) {
         const uint32_t wi = __ffs(nz) - 1;
         nz &= nz - 1;
-        cur = s.bm[tw0 + wi];
-        s.bm[tw0 + wi] = 0u;
+        cur = s.bm[wi * kRankThreads + tid];
+        s.bm[wi * kRankThreads + tid] = 0u;
         base = lo + ((tw0 + wi) << 5) - 1;
       }
       st[k] = (int32_t)(base + __ffs(cur));
@@ -625,8 +629,8 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
       if (cur == 0) {
         const uint32_t wi = __ffs(nz) - 1;
         nz &= nz - 1;
-        cur = s.bm[tw0 + wi];
-        s.bm[tw0 + wi] = 0u;
+        cur = s.bm[wi * kRankThreads + tid];
+        s.bm[wi * kRankThreads + tid] = 0u;
         base = lo + ((tw0 + wi) << 5) - 1;
       }
       dst[pos + k] = (int32_t)(base + __ffs(cur));
