@@ -183,25 +183,29 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
   }
   // hit-bit room in per-warp chunks of the global cursor (one atomic per
   // chunk, not per group); kNoMask once the cache's capacity is used up
-  uint32_t ch_pos = 0, ch_end = 0;
-  bool ch_out = false;
+  // (the warp's chunk is kept in shared memory, not in registers: the count
+  // pass is latency-bound and its occupancy is set by its registers)
+  __shared__ uint32_t chunk[8][2];  // per warp: next word, end (end = kNoMask: no room left)
+  if (lane == 0) chunk[wib][0] = chunk[wib][1] = 0;
+  __syncwarp();
   auto mask_alloc = [&](uint32_t want) -> uint32_t {
-    if (ch_pos + want > ch_end) {
-      if (ch_out) return kNoMask;
-      const uint32_t grab = want > kMaskChunk ? want : kMaskChunk;
-      uint32_t base = 0;
-      if (lane == 0) base = atomicAdd(hc.cursor, grab);
-      base = __shfl_sync(0xffffffffu, base, 0);
-      if ((uint64_t)base + grab > hc.mask_cap) {
-        ch_out = true;
-        return kNoMask;
+    uint32_t r = 0;
+    if (lane == 0) {
+      uint32_t pos = chunk[wib][0], end = chunk[wib][1];
+      if (end == kNoMask) {
+        r = kNoMask;
+      } else {
+        if (pos + want > end) {
+          const uint32_t grab = want > kMaskChunk ? want : kMaskChunk;
+          pos = atomicAdd(hc.cursor, grab);
+          end = ((uint64_t)pos + grab > hc.mask_cap) ? kNoMask : pos + grab;
+        }
+        r = (end == kNoMask) ? kNoMask : pos;
+        chunk[wib][0] = pos + want;
+        chunk[wib][1] = end;
       }
-      ch_pos = base;
-      ch_end = base + grab;
     }
-    const uint32_t r = ch_pos;
-    ch_pos += want;
-    return r;
+    return __shfl_sync(0xffffffffu, r, 0);
   };
   const uint32_t nitems = (uint32_t)min((uint64_t)*item_count, item_cap);
   const float* lmbr = t.mbr[0];
