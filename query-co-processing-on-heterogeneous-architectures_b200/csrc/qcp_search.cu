@@ -861,14 +861,14 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
       mark(ws, kEvWrite, s);
       if (sort) QCP_TRY(segmented_sort(ix, ws, q, s));
       mark(ws, kEvSort, s);
-      if (ws->leaf_ring >= 2) {
-        QCP_CUDA(cudaMemcpyAsync(ws->h_ctr + kCtrTimeout, ctr + kCtrTimeout, sizeof(uint32_t),
-                                 cudaMemcpyDeviceToHost, s));
-        QCP_CUDA(cudaStreamSynchronize(s));
-        if (ws->h_ctr[kCtrTimeout]) {
-          set_error("a bounded wait for a leaf's bulk copy ran out in the write pass");
-          return QCP_ERR_TIMEOUT;
-        }
+      // bounded waits of the write pass's leaf ring and the window sort's
+      // bulk prefetch
+      QCP_CUDA(cudaMemcpyAsync(ws->h_ctr + kCtrTimeout, ctr + kCtrTimeout, sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost, s));
+      QCP_CUDA(cudaStreamSynchronize(s));
+      if (ws->h_ctr[kCtrTimeout]) {
+        set_error("a bounded wait for a bulk copy ran out in the write pass or the sort");
+        return QCP_ERR_TIMEOUT;
       }
     }
     // hit bits that did not fit this call were tested again by the write

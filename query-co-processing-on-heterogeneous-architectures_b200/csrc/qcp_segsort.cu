@@ -471,11 +471,32 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
 // ============================================================================
 template <uint32_t BITS>
 struct RankSmem {
+  uint64_t bar;                             // completion of the window's bulk prefetch
+  uint64_t pad_;
   uint32_t bm[WinCfg<BITS>::kWords];        // one bit per possible id of the window
-  int32_t stage[WinCfg<BITS>::kStage];      // output positions [0, kStage) of the window
-  int32_t pf[WinCfg<BITS>::kPrefetch];      // first ids of the next window, loaded ahead
+  // output ranks [0, kStage) of the window, rank r at stage[r + (off & 3)] so
+  // that the stage and the output share their 16-byte alignment
+  int32_t stage[WinCfg<BITS>::kStage + 4];
+  // first ids of the next window, loaded ahead: id i of a window at offset
+  // off is at pf[i + (off & 3)]
+  int32_t pf[WinCfg<BITS>::kPrefetch + 4];
   uint32_t wsum[WinCfg<BITS>::kWarps];      // set bits in each warp's word range
 };
+
+// Shared -> global bulk copy (the TMA unit) of `bytes` (a multiple of 16,
+// both addresses 16-byte aligned), tracked as a bulk async-group.
+__device__ __forceinline__ void bulk_copy_s2g(void* gdst, const void* ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(gdst),
+               "r"(static_cast<uint32_t>(__cvta_generic_to_shared(ssrc))), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+// Until the issued bulk stores have read their shared-memory source.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+// Until the issued bulk stores are complete.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+// Generic-proxy writes to shared memory before async-proxy reads of them.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
 // 4-byte global -> shared copies that run behind the CTA's other work
 // (cp.async, waited for with cp_async_wait_all before the data is read).
@@ -509,7 +530,7 @@ template <uint32_t BITS>
 __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     k_win_sort(const uint32_t* __restrict__ njobs_p, uint32_t G, uint32_t wbits, const uint32_t* __restrict__ whist,
                const unsigned long long* __restrict__ wbase, const int32_t* __restrict__ src,
-               int32_t* __restrict__ out) {
+               int32_t* __restrict__ out, uint32_t* err) {
   using C = WinCfg<BITS>;
   constexpr uint32_t kRankThreads = C::kThreads;
   constexpr uint32_t kRankWarps = C::kWarps;
@@ -529,18 +550,41 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
   // that the lanes of a warp reading or clearing one word each of their own
   // ranges always hit 32 distinct banks.
   for (uint32_t i = tid; i < kBmWords / 4; i += kRankThreads) bm4[i] = make_uint4(0, 0, 0, 0);
+  if (tid == 0) {
+    mbar_init(&s.bar, 1);
+    mbar_fence_init();
+  }
   __syncthreads();
-  // the first kPrefetch ids of window g + gridDim.x are copied into s.pf
-  // while window g is enumerated
+  // The first kPrefetch ids of window g + gridDim.x are copied into s.pf
+  // while window g is enumerated: their 16-byte-aligned middle by one bulk
+  // copy (thread 0, completing on s.bar, one barrier phase per window even
+  // when it is empty), the up to 3 + 3 ids around it by cp.async.
+  auto prefetch = [&](unsigned long long o, uint32_t sz) {
+    const uint32_t n = sz < kPrefetch ? sz : kPrefetch;
+    const unsigned long long al = o & ~3ull;
+    const unsigned long long a0 = (o + 3) & ~3ull, a1 = (o + n) & ~3ull;
+    const bool bulk = a1 > a0;
+    if (tid == 0) {
+      mbar_arrive_expect_tx(&s.bar, bulk ? (uint32_t)(a1 - a0) * 4u : 0u);
+      if (bulk) bulk_copy_g2s(&s.pf[a0 - al], src + a0, (uint32_t)(a1 - a0) * 4u, &s.bar);
+    }
+    if (bulk) {
+      const uint32_t nh = (uint32_t)(a0 - o), nt = (uint32_t)(o + n - a1);
+      if (tid < nh) cp_async4(&s.pf[o - al + tid], src + o + tid);
+      else if (tid >= 4 && tid - 4 < nt) cp_async4(&s.pf[a1 - al + (tid - 4)], src + a1 + (tid - 4));
+    } else if (tid < n) {
+      cp_async4(&s.pf[o - al + tid], src + o + tid);
+    }
+    cp_async_commit();
+  };
+  uint32_t phase = 0;
   uint32_t size = 0;
   unsigned long long off = 0;
   if (blockIdx.x < total) {
     size = whist[blockIdx.x];
     off = wbase[blockIdx.x];
-    const uint32_t n = size < kPrefetch ? size : kPrefetch;
-    for (uint32_t i = tid; i < n; i += kRankThreads) cp_async4(&s.pf[i], src + off + i);
+    prefetch(off, size);
   }
-  cp_async_commit();
   for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
     const uint32_t gn = g + gridDim.x;
     uint32_t nsize = 0;
@@ -552,14 +596,26 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     const int32_t* in = src + off;
     int32_t* dst = out + off;
     const uint32_t lo = (g % G) << wbits;
+    const uint32_t sh = (uint32_t)(off & 3);  // 16-byte alignment offset of this window's ids
+    // this window's prefetched ids, and the stage free of the previous
+    // window's bulk store
+    const bool ok = mbar_wait_bounded(&s.bar, phase);
+    phase ^= 1u;
     cp_async_wait_all();
-    __syncthreads();  // this window's prefetched ids are visible to every thread
+    if (tid == 0) bulk_wait_read();
+    if (__syncthreads_or(!ok)) {
+      // a bulk copy did not complete in time: flag it and stop (the results
+      // are invalid); wait once more, again bounded, for that copy
+      if (tid == 0) atomicOr(err, 1u);
+      mbar_wait_bounded(&s.bar, phase ^ 1u);
+      break;
+    }
     // 1. set one bit per id: the prefetched ones from shared memory, the
     //    rest in rounds whose loads are all issued before the first atomic
     if (size >= 2) {
       const uint32_t npf = size < kPrefetch ? size : kPrefetch;
       for (uint32_t i = tid; i < npf; i += kRankThreads) {
-        const uint32_t x = (uint32_t)s.pf[i] - lo;
+        const uint32_t x = (uint32_t)s.pf[i + sh] - lo;
         atomicOr(&s.bm[bm_at<BITS>(x >> 5)], 1u << (x & 31));
       }
       for (uint32_t i0 = kPrefetch; i0 < size; i0 += kBatch * kRankThreads) {
@@ -576,14 +632,10 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
             atomicOr(&s.bm[bm_at<BITS>(a[k] >> 5)], 1u << (a[k] & 31));
       }
     } else if (size == 1 && tid == 0) {
-      dst[0] = s.pf[0];
+      dst[0] = s.pf[sh];
     }
     __syncthreads();  // bitmap complete; s.pf free
-    {
-      const uint32_t n = nsize < kPrefetch ? nsize : kPrefetch;
-      for (uint32_t i = tid; i < n; i += kRankThreads) cp_async4(&s.pf[i], src + noff + i);
-      cp_async_commit();
-    }
+    if (gn < total) prefetch(noff, nsize);
     if (size < 2) {
       size = nsize;
       off = noff;
@@ -613,7 +665,7 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     // iteration tests the rank.
     uint32_t cur = 0, base = 0;
     const uint32_t nst = pos < kStage ? min(cnt, kStage - pos) : 0u;
-    int32_t* st = s.stage + pos;
+    int32_t* st = s.stage + sh + pos;
     for (uint32_t k = 0; k < nst; ++k) {
       if (cur == 0) {
         const uint32_t wi = __ffs(nz) - 1;
@@ -636,14 +688,28 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
       dst[pos + k] = (int32_t)(base + __ffs(cur));
       cur &= cur - 1;
     }
+    fence_proxy_async_smem();  // the stage's writes before the bulk store reads them
     __syncthreads();
-    // 3. staged ranks out
+    // 3. staged ranks out: the 16-byte-aligned middle by one bulk store, the
+    //    up to 3 + 3 ids around it by plain stores
     const uint32_t ns = size < kStage ? size : kStage;
-    for (uint32_t k = tid; k < ns; k += kRankThreads) dst[k] = s.stage[k];
+    {
+      const unsigned long long al = off & ~3ull;
+      const unsigned long long b0 = (off + 3) & ~3ull, b1 = (off + ns) & ~3ull;
+      if (b1 > b0) {
+        if (tid == 0) bulk_copy_s2g(out + b0, &s.stage[b0 - al], (uint32_t)(b1 - b0) * 4u);
+        const uint32_t nh = (uint32_t)(b0 - off), nt = (uint32_t)(off + ns - b1);
+        if (tid < nh) out[off + tid] = s.stage[sh + tid];
+        else if (tid >= 4 && tid - 4 < nt) out[b1 + (tid - 4)] = s.stage[b1 - al + (tid - 4)];
+      } else {
+        for (uint32_t k = tid; k < ns; k += kRankThreads) dst[k] = s.stage[sh + k];
+      }
+    }
     size = nsize;
     off = noff;
   }
   cp_async_wait_all();
+  if (tid == 0) bulk_wait_all();
 }
 
 }  // namespace
@@ -674,19 +740,20 @@ static uint32_t id_bits(uint64_t n) {
 template <uint32_t BITS>
 static void launch_win_sort_t(uint64_t max_pairs, uint32_t sms, const uint32_t* njobs, uint32_t G, uint32_t wbits,
                               const uint32_t* whist, const unsigned long long* wbase, const int32_t* src,
-                              int32_t* out, cudaStream_t s) {
+                              int32_t* out, uint32_t* err, cudaStream_t s) {
   using C = WinCfg<BITS>;
   const uint64_t cap = (uint64_t)sms * C::kBlocks;
   const uint32_t grid = (uint32_t)(max_pairs < cap ? max_pairs : cap);
-  if (grid) k_win_sort<BITS><<<grid, C::kThreads, sizeof(RankSmem<BITS>), s>>>(njobs, G, wbits, whist, wbase, src, out);
+  if (grid)
+    k_win_sort<BITS><<<grid, C::kThreads, sizeof(RankSmem<BITS>), s>>>(njobs, G, wbits, whist, wbase, src, out, err);
 }
 
 static void launch_win_sort(uint64_t max_pairs, uint32_t sms, const uint32_t* njobs, uint32_t G, uint32_t wbits,
                             const uint32_t* whist, const unsigned long long* wbase, const int32_t* src, int32_t* out,
-                            cudaStream_t s) {
-  if (wbits >= 18) launch_win_sort_t<18>(max_pairs, sms, njobs, G, wbits, whist, wbase, src, out, s);
-  else if (wbits == 17) launch_win_sort_t<17>(max_pairs, sms, njobs, G, wbits, whist, wbase, src, out, s);
-  else launch_win_sort_t<16>(max_pairs, sms, njobs, G, wbits, whist, wbase, src, out, s);
+                            uint32_t* err, cudaStream_t s) {
+  if (wbits >= 18) launch_win_sort_t<18>(max_pairs, sms, njobs, G, wbits, whist, wbase, src, out, err, s);
+  else if (wbits == 17) launch_win_sort_t<17>(max_pairs, sms, njobs, G, wbits, whist, wbase, src, out, err, s);
+  else launch_win_sort_t<16>(max_pairs, sms, njobs, G, wbits, whist, wbase, src, out, err, s);
 }
 
 static qcp_status set_sort_attrs(const qcp_index* ix, size_t scatter_max) {
@@ -819,7 +886,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
         big, map, tile_off, ctr + kCtrWork2, ws->out_ids, ws->tmp_ids, G, wbits, wcur);
     mark(ws, kEvSortPart, s);
     ws->sort_part_marked = ws->timing;
-    launch_win_sort(nw, sms, ctr + kCtrJobs1, G, wbits, whist, wbase, ws->tmp_ids, ws->out_ids, s);
+    launch_win_sort(nw, sms, ctr + kCtrJobs1, G, wbits, whist, wbase, ws->tmp_ids, ws->out_ids, ctr + kCtrTimeout, s);
     note_launch(5);
     st = check_launch("segmented sort windows");
     // the tables go back to the pool below: make sure the kernels are done
@@ -903,7 +970,8 @@ qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void*
   k_win_scatter<<<sms * scatter_blocks_per_sm(scatter_bytes), kTileThreads, scatter_bytes, s>>>(
       big, ws->seg_hist, tile_off, ctr + kCtrWork2,
                                                              ws->out_ids, ws->tmp_ids, G, wbits, wcur);
-  launch_win_sort((uint64_t)-1, sms, ctr + kCtrJobs1, G, wbits, whist, wbase, ws->tmp_ids, ws->out_ids, s);
+  launch_win_sort((uint64_t)-1, sms, ctr + kCtrJobs1, G, wbits, whist, wbase, ws->tmp_ids, ws->out_ids,
+                  ctr + kCtrTimeout, s);
   note_launch(5);
   return check_launch("segmented sort (device counts)");
 }
