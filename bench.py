@@ -261,12 +261,13 @@ def run_ours(args, rank, world, local):
 
     # ---- autotune on a separate query sample of the same distribution -------
     knobs = {"fanout": args.fanout, "blocks_per_sm": args.blocks_per_sm, "win_bits": args.win_bits,
-             "leaf_prefetch": args.leaf_prefetch, "lanes_per_item": args.lanes_per_item}
+             "leaf_prefetch": args.leaf_prefetch, "lanes_per_item": args.lanes_per_item, "hit_cache": args.hit_cache}
     tune = None
     if args.algo == "batched" and not args.no_tune:
         sample = tune_sample(W, args.workload, w)
         tune = qcp.autotune(w.objs, sample, is_rect=w.is_rect, dims=w.dims, repeats=2)
-        knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch", "lanes_per_item")}
+        knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch", "lanes_per_item",
+                                      "hit_cache")}
     args.fanout = knobs["fanout"]
 
     t0 = time.perf_counter()
@@ -290,7 +291,8 @@ def run_ours(args, rank, world, local):
     def step_device(algo, timing):
         r = ix.search(d_boxes, q=Q, algo=algo, result_mem=qcp.MEM_DEVICE, stream=sp, timing=timing,
                       blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
-                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"])
+                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"],
+                    hit_cache=knobs["hit_cache"])
         hits = r.total_hits
         r.release()
         return hits
@@ -337,7 +339,8 @@ def run_ours(args, rank, world, local):
     # ---- parity of the timed batch (after the timed region) -----------------
     res = ix.search(d_boxes, q=Q, algo=args.algo, result_mem=qcp.MEM_DEVICE, stream=sp,
                     blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
-                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"])
+                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"],
+                    hit_cache=knobs["hit_cache"])
     got_counts, nchecked, fail = verify_result(res, Q, d_objs, d_boxes, w.dims, w.is_rect)
     res.release()
     parity = {"ids_checked": int(nchecked), "slices_ascending_and_in_box": fail is None}
@@ -363,7 +366,8 @@ def run_ours(args, rank, world, local):
         def step_unsorted(algo):
             r = ix.search(d_boxes, q=Q, algo=algo, sort=False, result_mem=qcp.MEM_DEVICE, stream=sp,
                           blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
-                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"])
+                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"],
+                    hit_cache=knobs["hit_cache"])
             r.release()
 
         plain = qps_of(lambda: step_device("plain", False))
@@ -387,7 +391,8 @@ def run_ours(args, rank, world, local):
     def step_host(st):
         r = ix.search(h_np, algo=args.algo, result_mem=qcp.MEM_HOST, stream=st.cuda_stream, copy=False,
                       blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
-                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"])
+                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"],
+                    hit_cache=knobs["hit_cache"])
         nb = (Q + 1) * 8 + r.total_hits * 4
         r.release()
         return nb
@@ -465,7 +470,8 @@ def run_ours(args, rank, world, local):
         plan_out = {}
         # (a) the timed batch itself through one plan
         with qcp.Plan(ix, Q, int(stats["hits"] * 1.05) + 1024, blocks_per_sm=knobs["blocks_per_sm"],
-                      win_bits=knobs["win_bits"], leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"]) as plan:
+                      win_bits=knobs["win_bits"], leaf_prefetch=knobs["leaf_prefetch"],
+                      lanes_per_item=knobs["lanes_per_item"]) as plan:
             plan.run_device(d_boxes, q=Q, stream=sp)
             torch.cuda.synchronize()
             e_a = torch.cuda.Event(enable_timing=True)
@@ -517,7 +523,8 @@ def run_ours(args, rank, world, local):
             for _ in range(args.steps):
                 ix.search(h_np, algo="hybrid", result_mem=qcp.MEM_DEVICE, stream=sp, handoff_level=h,
                           blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
-                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"]).release()
+                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"],
+                    hit_cache=knobs["hit_cache"]).release()
             e_b.record(stream)
             e_b.synchronize()
             hm = e_a.elapsed_time(e_b) / args.steps
@@ -601,11 +608,12 @@ def run_ours(args, rank, world, local):
             "win_bits": knobs["win_bits"] or 17,
             "leaf_prefetch": knobs["leaf_prefetch"] or 2,
             "lanes_per_item": knobs["lanes_per_item"] or 32,
+            "hit_cache": "off" if knobs["hit_cache"] == 1 else "on",
             "tuned": None if tune is None else {"sample_queries": 2000, "best_ms": round(tune["best_ms"], 3),
                                                 "trial_fields": ["fanout", "blocks_per_sm", "win_bits",
-                                                                 "leaf_prefetch", "lanes_per_item", "ms"],
+                                                                 "leaf_prefetch", "lanes_per_item", "hit_cache", "ms"],
                                                 "trials": [[t["fanout"], t["blocks_per_sm"], t["win_bits"],
-                                                            t["leaf_prefetch"], t["lanes_per_item"],
+                                                            t["leaf_prefetch"], t["lanes_per_item"], t["hit_cache"],
                                                             round(t["ms"], 3)] for t in tune["trials"]]},
             "algo": args.algo, "queries_per_step_per_gpu": Q,
             "n_objects": w.n, "key": f"hilbert {info['key_bits']} bits/dim",
@@ -701,11 +709,13 @@ def measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind):
     stream = torch.cuda.current_stream(dev)
     d_objs = torch.from_numpy(w.objs).to(dev)
     d_boxes = torch.from_numpy(boxes).to(dev)
-    knobs = {"fanout": 128, "blocks_per_sm": 0, "win_bits": 0, "leaf_prefetch": 0, "lanes_per_item": 0}
+    knobs = {"fanout": 128, "blocks_per_sm": 0, "win_bits": 0, "leaf_prefetch": 0, "lanes_per_item": 0,
+             "hit_cache": 0}
     tune = None
     if not args.no_tune:
         tune = qcp.autotune(w.objs, tune_sample(W, name, w), is_rect=w.is_rect, dims=w.dims, repeats=2)
-        knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch", "lanes_per_item")}
+        knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch", "lanes_per_item",
+                                      "hit_cache")}
     build = dict(fanout=knobs["fanout"], dims=w.dims, n=w.n, is_rect=w.is_rect, key_bits=w.key_bits, stream=sp)
     qcp.Index.build(d_objs, **build).close()  # warm-up build
     torch.cuda.synchronize()
@@ -719,7 +729,8 @@ def measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind):
     ix = qcp.Index.build(d_objs, **build)
     info = ix.info()
     kq = dict(blocks_per_sm=knobs["blocks_per_sm"], win_bits=knobs["win_bits"],
-                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"])
+                    leaf_prefetch=knobs["leaf_prefetch"], lanes_per_item=knobs["lanes_per_item"],
+                    hit_cache=knobs["hit_cache"])
 
     def step(algo, timing=False):
         r = ix.search(d_boxes, q=Q, algo=algo, result_mem=qcp.MEM_DEVICE, stream=sp, timing=timing, **kq)
@@ -790,7 +801,7 @@ def measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind):
            "steps": args.steps, "warmup": args.warmup, "hits_per_step": int(stats["hits"]),
            "knobs": knobs, "key": f"hilbert {info['key_bits']} bits/dim", "levels": info["levels"],
            "tuned": None if tune is None else [[t["fanout"], t["blocks_per_sm"], t["win_bits"], t["leaf_prefetch"],
-                                                t["lanes_per_item"], round(t["ms"], 3)]
+                                                t["lanes_per_item"], t["hit_cache"], round(t["ms"], 3)]
                                                for t in tune["trials"]],
            "phase_ms_per_step": {k: round(v / args.steps, 4) for k, v in phase.items()},
            "roofline": roof,
@@ -918,6 +929,7 @@ def main():
     ap.add_argument("--fanout", type=int, default=128)
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="traversal blocks per SM with --no-tune (0: default)")
     ap.add_argument("--win-bits", type=int, default=0, help="sort window bits with --no-tune (0: default)")
+    ap.add_argument("--hit-cache", type=int, default=0, help="with --no-tune: 0 = hit cache on, 1 = off")
     ap.add_argument("--lanes-per-item", type=int, default=0,
                     help="lanes per (query, node) item of the level expansion with --no-tune (0: 32)")
     ap.add_argument("--leaf-prefetch", type=int, default=0,

@@ -143,6 +143,12 @@ typedef struct qcp_query_opts {
    * that share one (query, node) item, 32 (default, 0), 16 or 8 (two or
    * four items per warp at once).  qcp_autotune picks it. */
   uint32_t lanes_per_item;
+  /* Hit cache between the two leaf passes of a call that writes ids: the
+   * count pass records which leaves overlap and which objects of partially
+   * covered leaves hit, and the write pass replays that instead of testing
+   * again.  0 = on (default), 1 = off (the count pass runs leaner, the write
+   * pass tests again).  qcp_autotune picks it. */
+  uint32_t hit_cache;
 } qcp_query_opts;
 
 /* flags: record CUDA events around every phase of the call; the times are
@@ -265,9 +271,9 @@ qcp_status qcp_query_counts_noalloc(qcp_index* index, const float* d_boxes, uint
  * win_bits, leaf_prefetch, lanes_per_item) for a data set and a sample of
  * its queries by timing trials on the current device: every fan-out in {64,
  * 128, 256} is built and queried with the default knobs, then blocks_per_sm
- * in {4, 8, 16}, win_bits in {16, 17, 18}, leaf_prefetch in {1, 2, 3} and
- * lanes_per_item in {8, 16, 32} are tried one after the other at the best
- * fan-out (coordinate descent); each trial is the median of `repeats` timed batches of the
+ * in {4, 8, 16}, win_bits in {16, 17, 18}, leaf_prefetch in {1, 2, 3},
+ * lanes_per_item in {8, 16, 32} and hit_cache on/off are tried one after
+ * the other at the best fan-out (coordinate descent); each trial is the median of `repeats` timed batches of the
  * sample (sorted output) after one untimed batch.  objs and boxes are host
  * memory as for qcp_index_build / qcp_query_batch; `base` supplies the key
  * mode, key bits and stream (its fanout is ignored).  The reference fixes
@@ -289,6 +295,8 @@ typedef struct qcp_tune_result {
   uint32_t trial_leaf_prefetch[QCP_TUNE_MAX_TRIALS];
   uint32_t lanes_per_item;    /* best qcp_query_opts.lanes_per_item */
   uint32_t trial_lanes_per_item[QCP_TUNE_MAX_TRIALS];
+  uint32_t hit_cache;         /* best qcp_query_opts.hit_cache */
+  uint32_t trial_hit_cache[QCP_TUNE_MAX_TRIALS];
 } qcp_tune_result;
 
 qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims, uint32_t is_rect, const float* boxes,

@@ -58,7 +58,8 @@ class QueryOpts(ctypes.Structure):
                 ("stream", ctypes.c_void_p), ("flags", ctypes.c_uint32),
                 ("blocks_per_sm", ctypes.c_uint32), ("win_bits", ctypes.c_uint32),
                 ("cpu_threads", ctypes.c_uint32), ("handoff_level", ctypes.c_uint32),
-                ("leaf_prefetch", ctypes.c_uint32), ("lanes_per_item", ctypes.c_uint32)]
+                ("leaf_prefetch", ctypes.c_uint32), ("lanes_per_item", ctypes.c_uint32),
+                ("hit_cache", ctypes.c_uint32)]
 
 
 QUERY_TIMING = 1
@@ -122,7 +123,9 @@ class TuneResult(ctypes.Structure):
                 ("leaf_prefetch", ctypes.c_uint32),
                 ("trial_leaf_prefetch", ctypes.c_uint32 * TUNE_MAX_TRIALS),
                 ("lanes_per_item", ctypes.c_uint32),
-                ("trial_lanes_per_item", ctypes.c_uint32 * TUNE_MAX_TRIALS)]
+                ("trial_lanes_per_item", ctypes.c_uint32 * TUNE_MAX_TRIALS),
+                ("hit_cache", ctypes.c_uint32),
+                ("trial_hit_cache", ctypes.c_uint32 * TUNE_MAX_TRIALS)]
 
 
 class Result(ctypes.Structure):
@@ -319,16 +322,17 @@ class Index:
 
     # -- queries --------------------------------------------------------------
     def _opts(self, algo, boxes_mem, result_mem, sort, stream, timing=False, blocks_per_sm=0, win_bits=0,
-              cpu_threads=0, handoff_level=0, leaf_prefetch=0, lanes_per_item=0):
+              cpu_threads=0, handoff_level=0, leaf_prefetch=0, lanes_per_item=0, hit_cache=0):
         a = {"batched": ALGO_BATCHED, "plain": ALGO_PLAIN, "hybrid": ALGO_HYBRID}.get(algo, algo)
         return QueryOpts(a, boxes_mem, result_mem, 0 if sort else 1, ctypes.c_void_p(stream or None),
                          QUERY_TIMING if timing else 0, blocks_per_sm, win_bits, cpu_threads, handoff_level,
-                         leaf_prefetch, lanes_per_item)
+                         leaf_prefetch, lanes_per_item, hit_cache)
 
     def search(self, boxes, algo="batched", sort: bool = True, result_mem: int = MEM_HOST,
                q: int | None = None, stream: int = 0, timing: bool = False,
                copy: bool = True, blocks_per_sm: int = 0, win_bits: int = 0, cpu_threads: int = 0,
-               handoff_level: int = 0, leaf_prefetch: int = 0, lanes_per_item: int = 0) -> SearchResult:
+               handoff_level: int = 0, leaf_prefetch: int = 0, lanes_per_item: int = 0,
+               hit_cache: int = 0) -> SearchResult:
         """Run a batch of box queries.  Host numpy boxes (q x 2D) or a CUDA
         tensor/pointer (then pass q).  Host results are copied into numpy
         arrays (copy=False: numpy views of the library's pinned result arena,
@@ -343,7 +347,7 @@ class Index:
                 raise ValueError("device boxes need q")
             b, nq, ptr, bmem = boxes, q, ctypes.c_void_p(_device_ptr(boxes)), MEM_DEVICE
         opts = self._opts(algo, bmem, result_mem, sort, stream, timing, blocks_per_sm, win_bits, cpu_threads,
-                          handoff_level, leaf_prefetch, lanes_per_item)
+                          handoff_level, leaf_prefetch, lanes_per_item, hit_cache)
         r = Result()
         _check(lib.qcp_query_batch(self._h, ptr, nq, ctypes.byref(opts), ctypes.byref(r)))
         if result_mem == MEM_HOST and not copy:
@@ -539,11 +543,12 @@ def autotune(objs, boxes, is_rect: bool = False, dims: int | None = None, key_mo
                                        ctypes.byref(bo), repeats, ctypes.byref(r)))
     n = r.trials
     return {"fanout": r.fanout, "blocks_per_sm": r.blocks_per_sm, "win_bits": r.win_bits,
-            "leaf_prefetch": r.leaf_prefetch, "lanes_per_item": r.lanes_per_item,
+            "leaf_prefetch": r.leaf_prefetch, "lanes_per_item": r.lanes_per_item, "hit_cache": r.hit_cache,
             "best_ms": r.best_ms, "build_ms": r.build_ms,
             "trials": [{"fanout": r.trial_fanout[i], "blocks_per_sm": r.trial_blocks_per_sm[i],
                         "win_bits": r.trial_win_bits[i], "leaf_prefetch": r.trial_leaf_prefetch[i],
-                        "lanes_per_item": r.trial_lanes_per_item[i], "ms": r.trial_ms[i]} for i in range(n)]}
+                        "lanes_per_item": r.trial_lanes_per_item[i], "hit_cache": r.trial_hit_cache[i],
+                        "ms": r.trial_ms[i]} for i in range(n)]}
 
 
 def last_stats() -> dict:

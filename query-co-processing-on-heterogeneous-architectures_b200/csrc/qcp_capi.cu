@@ -580,6 +580,7 @@ static qcp_status run_query(qcp_index* ix, const float* boxes, uint32_t q, const
   ws->win_bits = o.win_bits ? (o.win_bits < 12 ? 12u : o.win_bits) : kDefaultWinBits;
   ws->leaf_ring = leaf_ring_of(o.leaf_prefetch);
   ws->lanes_per_item = lanes_per_item_of(o.lanes_per_item);
+  ws->hit_cache_on = o.hit_cache != 1;
   ws->sort_small_jobs = ws->sort_msd_jobs = 0;
   ws->hybrid = o.algo == QCP_ALGO_HYBRID;
   ws->cpu_threads = o.cpu_threads;

@@ -124,6 +124,7 @@ struct Workspace {
   uint32_t* hmask = nullptr;
   size_t hmask_cap = 0;          // words
   bool use_hit_cache = false;    // this call's count pass fills the cache
+  bool hit_cache_on = true;      // qcp_query_opts.hit_cache of this call
   uint32_t lanes_per_item = 32;  // lanes of k_expand per (query, node) item, this call
   // CPU + GPU co-processing (QCP_ALGO_HYBRID) of this call
   bool hybrid = false;

@@ -139,7 +139,7 @@ constexpr uint32_t kMaskChunk = 1024;  // hit-cache words a warp takes at a time
 // leaves ahead, completion on one mbarrier per buffer) while the warp tests
 // the leaf before; without PF every lane loads its float4s from global
 // memory.  A bulk-copy wait that runs out sets err[0] and the warp stops.
-template <int D, bool RECT, int MODE, bool PF>
+template <int D, bool RECT, int MODE, bool PF, bool CACHE>
 __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __restrict__ boxes,
                                                   const uint2* __restrict__ items,
                                                   const uint32_t* __restrict__ item_count,
@@ -186,8 +186,10 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
   // (the warp's chunk is kept in shared memory, not in registers: the count
   // pass is latency-bound and its occupancy is set by its registers)
   __shared__ uint32_t chunk[8][2];  // per warp: next word, end (end = kNoMask: no room left)
-  if (lane == 0) chunk[wib][0] = chunk[wib][1] = 0;
-  __syncwarp();
+  if (CACHE) {
+    if (lane == 0) chunk[wib][0] = chunk[wib][1] = 0;
+    __syncwarp();
+  }
   auto mask_alloc = [&](uint32_t want) -> uint32_t {
     uint32_t r = 0;
     if (lane == 0) {
@@ -230,7 +232,7 @@ __global__ void __launch_bounds__(256) k_leafscan(TreeView t, const float* __res
     uint32_t npart = 0;  // PF: partially covered leaves listed for the ring
     const uint64_t l0 = (uint64_t)it.y * F;
     const uint64_t l1 = (l0 + F < nleaves) ? l0 + F : nleaves;
-    const bool cache = hc.grp != nullptr;
+    const bool cache = CACHE && hc.grp != nullptr;
     const uint32_t wpl = words_per_leaf(F);
     uint32_t* grec = cache ? hc.grp + (size_t)i * (kMaxGroups * kGrpWords) : nullptr;
     uint32_t g_mov = 0, g_min = 0;  // ring path: lane g holds group g's masks
@@ -675,9 +677,11 @@ void launch_leafscan_t(uint32_t grid, cudaStream_t s, const TreeView& t, const f
                        unsigned long long* stats, uint32_t* qwhist, uint32_t hist_G, uint32_t hist_bits,
                        uint32_t ring, uint32_t* err, HitCache hc) {
   const uint32_t nb = ring_buffers(leaf_runs(D, RECT, MODE), t.fanout, ring);
+  // the hit-cache code costs registers (occupancy of a latency-bound pass):
+  // calls without a cache run an instantiation without it
   if (nb) {
     const size_t smem = 8u * (size_t)ring_warp_bytes(leaf_runs(D, RECT, MODE), t.fanout, nb);
-    auto* kern = k_leafscan<D, RECT, MODE, true>;
+    auto* kern = hc.grp ? k_leafscan<D, RECT, MODE, true, true> : k_leafscan<D, RECT, MODE, true, false>;
     if (smem > 48u * 1024u) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // no more CTAs than fit on the SMs at once (the static counters and 1 KB
     // per CTA of reserved shared memory included)
@@ -689,10 +693,10 @@ void launch_leafscan_t(uint32_t grid, cudaStream_t s, const TreeView& t, const f
                                  (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap,
                                  stats, qwhist, hist_G, hist_bits, nb, err, hc);
   } else {
-    k_leafscan<D, RECT, MODE, false><<<grid, 256, 0, s>>>(
-        t, boxes, items, item_count, work, item_hits, (unsigned long long*)qcount,
-        (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap, stats, qwhist, hist_G,
-        hist_bits, 0u, err, hc);
+    auto* kern = hc.grp ? k_leafscan<D, RECT, MODE, false, true> : k_leafscan<D, RECT, MODE, false, false>;
+    kern<<<grid, 256, 0, s>>>(t, boxes, items, item_count, work, item_hits, (unsigned long long*)qcount,
+                              (const unsigned long long*)offsets, (unsigned long long*)qcursor, out, item_cap, stats,
+                              qwhist, hist_G, hist_bits, 0u, err, hc);
   }
 }
 
@@ -814,7 +818,7 @@ qcp_status run_batched(qcp_index* ix, Workspace* ws, uint32_t q, bool counts_onl
     // the level-1 items must fit the per-item hit array too
     QCP_TRY(ws_reserve_items(ix, ws, 0));
     // a call that writes ids keeps the count pass's hits for the write pass
-    ws->use_hit_cache = !counts_only;
+    ws->use_hit_cache = !counts_only && ws->hit_cache_on;
     if (ws->use_hit_cache) QCP_TRY(ws_reserve_hitcache(ws, ws->items_cap, ws->hmask_cap ? 0 : (size_t)1 << 20));
     QCP_DISPATCH_D(D, launch_leafscan<DD, kCount>(rect, grid, s, t, ws->boxes, ws->items[cur],
                                                   ctr + kCtrFrontier0 + cur, ctr + kCtrWork,

@@ -17,10 +17,13 @@
 //                  shared-memory ring (bulk copies), or none, which trades
 //                  latency hiding against CTAs per SM;
 //   lanes_per_item queries per warp of the level expansion: 32, 16 or 8
-//                  lanes per (query, node) item.
+//                  lanes per (query, node) item;
+//   hit_cache      the count pass's leaf masks and hit bits replayed by the
+//                  write pass, or both passes testing (a leaner count pass).
 // Search: coordinate descent -- fan-out first (every candidate built and
 // queried with default knobs), then blocks_per_sm, then win_bits, then
-// leaf_prefetch, then lanes_per_item, each at the best values found so far.  A trial is the median of `repeats` timed
+// leaf_prefetch, then lanes_per_item, then hit_cache, each at the best values
+// found so far.  A trial is the median of `repeats` timed
 // batches after one untimed batch, timed with CUDA events on the call's
 // stream, sorted output left on the device.
 #include <algorithm>
@@ -37,7 +40,7 @@ struct Trial {
 };
 
 Trial time_batch(qcp_index* ix, const float* d_boxes, uint32_t q, cudaStream_t s, uint32_t bps, uint32_t wb,
-                 uint32_t lp, uint32_t lpi, uint32_t repeats, cudaEvent_t e0, cudaEvent_t e1) {
+                 uint32_t lp, uint32_t lpi, uint32_t hcache, uint32_t repeats, cudaEvent_t e0, cudaEvent_t e1) {
   Trial tr;
   qcp_query_opts o;
   memset(&o, 0, sizeof(o));
@@ -48,6 +51,7 @@ Trial time_batch(qcp_index* ix, const float* d_boxes, uint32_t q, cudaStream_t s
   o.win_bits = wb;
   o.leaf_prefetch = lp;
   o.lanes_per_item = lpi;
+  o.hit_cache = hcache;
   std::vector<float> ms;
   for (uint32_t r = 0; r <= repeats; ++r) {
     qcp_result res;
@@ -96,10 +100,11 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
       st = qcp::cuda_status(cudaGetLastError(), "qcp_autotune setup");
       break;
     }
-    uint32_t best_lpi = 32;
+    uint32_t best_lpi = 32, best_hc = 0;
     auto record = [&](uint32_t f, uint32_t b, uint32_t w, uint32_t lp, float ms) {
       if (out->trials < QCP_TUNE_MAX_TRIALS) {
         out->trial_lanes_per_item[out->trials] = best_lpi;
+        out->trial_hit_cache[out->trials] = best_hc;
         out->trial_fanout[out->trials] = f;
         out->trial_blocks_per_sm[out->trials] = b;
         out->trial_win_bits[out->trials] = w;
@@ -120,7 +125,7 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
       const float build_ms =
           std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
       if (st != QCP_OK) break;
-      const Trial tr = time_batch(ix, (const float*)d_boxes, q, s, best_b, best_w, best_lp, best_lpi, repeats, e0, e1);
+      const Trial tr = time_batch(ix, (const float*)d_boxes, q, s, best_b, best_w, best_lp, best_lpi, best_hc, repeats, e0, e1);
       if (tr.st != QCP_OK) {
         st = tr.st;
         qcp_index_free(ix);
@@ -140,7 +145,7 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
     if (st != QCP_OK) break;
     // 2. blocks per SM, then 3. sort window bits, at the best so far
     for (uint32_t b : {4u, 16u}) {
-      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, b, best_w, best_lp, best_lpi, repeats, e0, e1);
+      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, b, best_w, best_lp, best_lpi, best_hc, repeats, e0, e1);
       if ((st = tr.st) != QCP_OK) break;
       record(best_f, b, best_w, best_lp, tr.ms);
       if (tr.ms < best) {
@@ -152,7 +157,7 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
     const uint32_t first_w = best_w;
     for (uint32_t w : {16u, 17u, 18u}) {
       if (w == first_w) continue;
-      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, best_b, w, best_lp, best_lpi, repeats, e0, e1);
+      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, best_b, w, best_lp, best_lpi, best_hc, repeats, e0, e1);
       if ((st = tr.st) != QCP_OK) break;
       record(best_f, best_b, w, best_lp, tr.ms);
       if (tr.ms < best) {
@@ -163,7 +168,7 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
     if (st != QCP_OK) break;
     // 4. leaf tile: no ring (1), or 3 buffers per warp instead of 2
     for (uint32_t lp : {1u, 3u}) {
-      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, best_b, best_w, lp, best_lpi, repeats, e0, e1);
+      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, best_b, best_w, lp, best_lpi, best_hc, repeats, e0, e1);
       if ((st = tr.st) != QCP_OK) break;
       record(best_f, best_b, best_w, lp, tr.ms);
       if (tr.ms < best) {
@@ -174,7 +179,7 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
     if (st != QCP_OK) break;
     // 5. queries per warp of the level expansion
     for (uint32_t lpi : {16u, 8u}) {
-      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, best_b, best_w, best_lp, lpi, repeats, e0, e1);
+      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, best_b, best_w, best_lp, lpi, best_hc, repeats, e0, e1);
       if ((st = tr.st) != QCP_OK) break;
       const uint32_t keep = best_lpi;
       best_lpi = lpi;
@@ -186,6 +191,20 @@ extern "C" qcp_status qcp_autotune(const float* objs, uint64_t n, uint32_t dims,
       }
     }
     if (st != QCP_OK) break;
+    // 6. the hit cache off
+    {
+      const Trial tr = time_batch(best_ix, (const float*)d_boxes, q, s, best_b, best_w, best_lp, best_lpi, 1u, repeats,
+                                  e0, e1);
+      if ((st = tr.st) != QCP_OK) break;
+      best_hc = 1;
+      record(best_f, best_b, best_w, best_lp, tr.ms);
+      best_hc = 0;
+      if (tr.ms < best) {
+        best = tr.ms;
+        best_hc = 1;
+      }
+    }
+    out->hit_cache = best_hc;
     out->lanes_per_item = best_lpi;
     out->fanout = best_f;
     out->leaf_prefetch = best_lp;

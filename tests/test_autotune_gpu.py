@@ -30,6 +30,8 @@ def test_knobs_keep_hits_exact(qcp, data, bps, wb, lp, lpi):
     with qcp.Index.build(objs, fanout=64) as ix:
         res = ix.search(boxes, blocks_per_sm=bps, win_bits=wb, leaf_prefetch=lp, lanes_per_item=lpi)
         assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
+        res = ix.search(boxes, blocks_per_sm=bps, win_bits=wb, leaf_prefetch=lp, lanes_per_item=lpi, hit_cache=1)
+        assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
         assert np.array_equal(ix.counts(boxes, leaf_prefetch=lp, lanes_per_item=lpi), np.diff(want_offs))
 
 
@@ -88,13 +90,14 @@ def test_autotune_choice_and_trials(qcp, data):
     assert r["win_bits"] in (16, 17, 18)
     assert r["leaf_prefetch"] in (1, 2, 3)
     assert r["lanes_per_item"] in (8, 16, 32)
-    # 3 fan-outs, 2 more grids, 2 more windows, 2 more leaf tiles, 2 more lane widths
-    assert len(r["trials"]) == 11
+    assert r["hit_cache"] in (0, 1)
+    # 3 fan-outs, 2 more grids, 2 more windows, 2 more leaf tiles, 2 more lane widths, the cache off
+    assert len(r["trials"]) == 12
     assert r["best_ms"] == pytest.approx(min(t["ms"] for t in r["trials"]))
     chosen = [t for t in r["trials"] if t["ms"] == r["best_ms"]][0]
-    keys = ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch", "lanes_per_item")
+    keys = ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch", "lanes_per_item", "hit_cache")
     assert tuple(chosen[k] for k in keys) == tuple(r[k] for k in keys)
     with qcp.Index.build(objs, fanout=r["fanout"]) as ix:
         res = ix.search(boxes, blocks_per_sm=r["blocks_per_sm"], win_bits=r["win_bits"],
-                        leaf_prefetch=r["leaf_prefetch"], lanes_per_item=r["lanes_per_item"])
+                        leaf_prefetch=r["leaf_prefetch"], lanes_per_item=r["lanes_per_item"], hit_cache=r["hit_cache"])
         assert_same_hits(res.offsets, res.ids, want_offs, want_ids)
