@@ -498,15 +498,6 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // Generic-proxy writes to shared memory before async-proxy reads of them.
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
-// 4-byte global -> shared copies that run behind the CTA's other work
-// (cp.async, waited for with cp_async_wait_all before the data is read).
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
 // Position of bitmap word w in shared memory (see k_win_sort).
 template <uint32_t BITS>
 __device__ __forceinline__ uint32_t bm_at(uint32_t w) {
@@ -516,16 +507,20 @@ __device__ __forceinline__ uint32_t bm_at(uint32_t w) {
 // Persistent CTAs over the (job, window) pairs g = job * G + window.
 //   1. every id of window g (read from src, the scratch buffer) sets its bit
 //      in a bitmap of the window's 2^wbits possible ids; its first kPrefetch
-//      ids were copied to shared memory while the previous window ran;
-//   2. every thread owns kLaneWords consecutive bitmap words: it counts their
-//      set bits, takes its exclusive prefix over the CTA (warp scan + warp
-//      sums), then walks its nonzero words in order and emits the id of
-//      every set bit at the next rank, clearing each word it read;
-//      ranks below kStage go to a shared-memory stage, larger ones straight
-//      to the output;
-//   3. the stage leaves in coalesced stores.
-// The ids of a window are distinct, so the set bits are the window's ids
-// and their enumeration in bit order is the window in ascending order.
+//      ids were brought into shared memory by a bulk copy (the TMA unit)
+//      while the previous window ran;
+//   2. every thread owns kLaneWords bitmap words: it counts their set bits,
+//      takes its exclusive prefix over the CTA (warp scan + warp sums), then
+//      walks its nonzero words in order and emits the id of every set bit at
+//      the next rank, clearing each word it read; ranks below kStage go to a
+//      shared-memory stage, larger ones straight to the output;
+//   3. the stage leaves by one bulk store (its 16-byte-aligned middle) and a
+//      few plain stores (the ends).
+// Three CTA barriers per window: bitmap complete, warp sums ready, stage
+// complete (which also orders the bitmap's clearing before the next
+// window's bits).  The ids of a window are distinct, so the set bits are the
+// window's ids and their enumeration in bit order is the window in
+// ascending order.
 template <uint32_t BITS>
 __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     k_win_sort(const uint32_t* __restrict__ njobs_p, uint32_t G, uint32_t wbits, const uint32_t* __restrict__ whist,
@@ -556,26 +551,25 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
   }
   __syncthreads();
   // The first kPrefetch ids of window g + gridDim.x are copied into s.pf
-  // while window g is enumerated: their 16-byte-aligned middle by one bulk
-  // copy (thread 0, completing on s.bar, one barrier phase per window even
-  // when it is empty), the up to 3 + 3 ids around it by cp.async.
-  auto prefetch = [&](unsigned long long o, uint32_t sz) {
+  // while window g is enumerated: their 16-byte-aligned middle [a0, a1) by
+  // one bulk copy (thread 0, completing on s.bar, one barrier phase per
+  // window even when it is empty); the up to 3 + 3 ids around it are read
+  // from global memory when the bits are set.  Every thread waits on s.bar
+  // itself, so the prefetched ids need no CTA barrier.
+  auto prefetch_range = [&](unsigned long long o, uint32_t sz, unsigned long long* a0,
+                            unsigned long long* a1) {
     const uint32_t n = sz < kPrefetch ? sz : kPrefetch;
-    const unsigned long long al = o & ~3ull;
-    const unsigned long long a0 = (o + 3) & ~3ull, a1 = (o + n) & ~3ull;
-    const bool bulk = a1 > a0;
+    *a0 = (o + 3) & ~3ull;
+    *a1 = (o + n) & ~3ull;
+    if (*a1 < *a0) *a1 = *a0;
+  };
+  auto prefetch = [&](unsigned long long o, uint32_t sz) {
+    unsigned long long a0, a1;
+    prefetch_range(o, sz, &a0, &a1);
     if (tid == 0) {
-      mbar_arrive_expect_tx(&s.bar, bulk ? (uint32_t)(a1 - a0) * 4u : 0u);
-      if (bulk) bulk_copy_g2s(&s.pf[a0 - al], src + a0, (uint32_t)(a1 - a0) * 4u, &s.bar);
+      mbar_arrive_expect_tx(&s.bar, (uint32_t)(a1 - a0) * 4u);
+      if (a1 > a0) bulk_copy_g2s(&s.pf[a0 - (o & ~3ull)], src + a0, (uint32_t)(a1 - a0) * 4u, &s.bar);
     }
-    if (bulk) {
-      const uint32_t nh = (uint32_t)(a0 - o), nt = (uint32_t)(o + n - a1);
-      if (tid < nh) cp_async4(&s.pf[o - al + tid], src + o + tid);
-      else if (tid >= 4 && tid - 4 < nt) cp_async4(&s.pf[a1 - al + (tid - 4)], src + a1 + (tid - 4));
-    } else if (tid < n) {
-      cp_async4(&s.pf[o - al + tid], src + o + tid);
-    }
-    cp_async_commit();
   };
   uint32_t phase = 0;
   uint32_t size = 0;
@@ -597,25 +591,21 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     int32_t* dst = out + off;
     const uint32_t lo = (g % G) << wbits;
     const uint32_t sh = (uint32_t)(off & 3);  // 16-byte alignment offset of this window's ids
-    // this window's prefetched ids, and the stage free of the previous
-    // window's bulk store
+    // this window's prefetched ids (every thread waits itself; the bitmap
+    // was cleared and the stage written before the previous window's last
+    // barrier), and the stage free of the previous window's bulk store
     const bool ok = mbar_wait_bounded(&s.bar, phase);
     phase ^= 1u;
-    cp_async_wait_all();
     if (tid == 0) bulk_wait_read();
-    if (__syncthreads_or(!ok)) {
-      // a bulk copy did not complete in time: flag it and stop (the results
-      // are invalid); wait once more, again bounded, for that copy
-      if (tid == 0) atomicOr(err, 1u);
-      mbar_wait_bounded(&s.bar, phase ^ 1u);
-      break;
-    }
     // 1. set one bit per id: the prefetched ones from shared memory, the
     //    rest in rounds whose loads are all issued before the first atomic
-    if (size >= 2) {
+    if (size >= 2 && ok) {
       const uint32_t npf = size < kPrefetch ? size : kPrefetch;
+      unsigned long long a0, a1;
+      prefetch_range(off, size, &a0, &a1);
+      const uint32_t i0 = (uint32_t)(a0 - off), i1 = (uint32_t)(a1 - off);  // [i0, i1) in s.pf
       for (uint32_t i = tid; i < npf; i += kRankThreads) {
-        const uint32_t x = (uint32_t)s.pf[i + sh] - lo;
+        const uint32_t x = (uint32_t)((i >= i0 && i < i1) ? s.pf[i + sh] : __ldcs(in + i)) - lo;
         atomicOr(&s.bm[bm_at<BITS>(x >> 5)], 1u << (x & 31));
       }
       for (uint32_t i0 = kPrefetch; i0 < size; i0 += kBatch * kRankThreads) {
@@ -632,9 +622,15 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
             atomicOr(&s.bm[bm_at<BITS>(a[k] >> 5)], 1u << (a[k] & 31));
       }
     } else if (size == 1 && tid == 0) {
-      dst[0] = s.pf[sh];
+      dst[0] = in[0];
     }
-    __syncthreads();  // bitmap complete; s.pf free
+    if (__syncthreads_or(!ok)) {  // bitmap complete; s.pf free
+      // a bulk copy did not complete in time: flag it and stop (the results
+      // are invalid); wait once more, again bounded, for that copy
+      if (tid == 0) atomicOr(err, 1u);
+      mbar_wait_bounded(&s.bar, phase ^ 1u);
+      break;
+    }
     if (gn < total) prefetch(noff, nsize);
     if (size < 2) {
       size = nsize;
@@ -708,7 +704,6 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     size = nsize;
     off = noff;
   }
-  cp_async_wait_all();
   if (tid == 0) bulk_wait_all();
 }
 
