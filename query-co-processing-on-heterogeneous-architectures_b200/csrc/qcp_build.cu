@@ -41,10 +41,22 @@ __device__ __forceinline__ int64_t quantise(float p, uint32_t bits, uint32_t mod
 }
 
 // One thread per object, the dimension count a template parameter so that
-// the coordinates and the key's bit levels stay in registers.
+// the coordinates and the key's bit levels stay in registers.  For D = 2 and
+// 3 each block first fills a shared-memory table of HilbertTab<D>::L levels
+// per lookup (3 KB, 1.5 KB), so a 2-D key takes 8 lookups instead of 32
+// level steps.
 template <int D>
 __global__ void k_keys(const float* __restrict__ objs, uint64_t n, uint32_t is_rect, uint32_t mode,
                        uint32_t bits, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  constexpr bool kTab = D == 2 || D == 3;
+  constexpr uint32_t kTabSize = kTab ? (HilbertTab<(D == 2 || D == 3) ? D : 2>::kStates
+                                        << (HilbertTab<(D == 2 || D == 3) ? D : 2>::L * D))
+                                     : 1u;
+  __shared__ uint16_t tab[kTabSize];
+  if constexpr (kTab) {
+    for (uint32_t e = threadIdx.x; e < kTabSize; e += blockDim.x) tab[e] = hilbert_tab_entry<D>(e);
+    __syncthreads();
+  }
   const uint32_t stride = is_rect ? 2 * D : D;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
@@ -55,7 +67,8 @@ __global__ void k_keys(const float* __restrict__ objs, uint64_t n, uint32_t is_r
       float p = is_rect ? __fmul_rn(0.5f, __fadd_rn(__ldg(o + d), __ldg(o + D + d))) : __ldg(o + d);
       c[d] = quantise(p, bits, mode);
     }
-    keys[i] = hilbert_index_t<D>(bits, c);
+    if constexpr (kTab) keys[i] = hilbert_index_tab<D>(bits, c, tab);
+    else keys[i] = hilbert_index_t<D>(bits, c);
     vals[i] = (uint32_t)i;
   }
 }

@@ -257,50 +257,115 @@ __host__ __device__ __forceinline__ uint64_t dilate(uint64_t x, uint32_t bits) {
 
 // Hilbert index of integer coordinates, the algorithm of
 // HilbertMapper::MappingIntoSingle (src/mapper/hilbert_mapper.cpp:25-64) and
-// hilbert_macro.h:4-22, written in unsigned 64-bit arithmetic: the
-// coordinates are packed (coordinate d at bits [d*bits, (d+1)*bits), wider
-// values spilling into the next field as in the reference's shifts), the
-// fields are transposed into bit levels (level b holds bit b of every
-// coordinate, coordinate d at bit d), then Gray-coded level by level with the
-// entry-point rotation, and prefix-XORed.
+// hilbert_macro.h:4-22, written in unsigned 64-bit arithmetic in three
+// parts: the coordinates are packed (coordinate d at bits [d*bits,
+// (d+1)*bits), wider values spilling into the next field as in the
+// reference's shifts) and transposed into bit levels (level b holds bit b of
+// every coordinate, coordinate d at bit d), the levels are Gray-coded from
+// the top with the entry-point rotation (one hilbert_step per level), and
+// the result is prefix-XORed.
+template <int D>
+__host__ __device__ __forceinline__ uint64_t hilbert_transpose(uint32_t bits, const int64_t* coord) {
+  uint64_t packed = 0;
+  for (int d = D - 1; d >= 0; --d) packed = (packed << bits) | (uint64_t)coord[d];
+  uint64_t t = 0;
+  const uint64_t field = low_ones64(bits);
+  for (uint32_t d = 0; d < (uint32_t)D; ++d) t |= dilate<D>((packed >> (d * bits)) & field, bits) << d;
+  return t;
+}
+
+// One level: gin = the level's D transposed bits; (rot, flip) the rotation
+// state carried from the level above (0, 0 at the top).  Returns the level's
+// D index bits.
+template <int D>
+__host__ __device__ __forceinline__ uint64_t hilbert_step(uint64_t gin, uint32_t& rot, uint64_t& flip) {
+  constexpr uint64_t nd_ones = (1ull << D) - 1ull;
+  constexpr uint64_t nd1_ones = nd_ones >> 1;
+  uint64_t g = gin ^ flip;
+  if (rot) g = ((g >> rot) | (g << (D - rot))) & nd_ones;
+  flip = 1ull << rot;
+  // the rotation advances past the lowest set bit of g below the top one
+  const uint64_t low = g & (0ull - g) & nd1_ones;
+  if (low) rot += 64u - clz64(low);
+  if (++rot >= (uint32_t)D) rot -= D;
+  return g;
+}
+
+template <int D>
+__host__ __device__ __forceinline__ uint64_t hilbert_finish(uint64_t index, uint32_t bits) {
+  const uint32_t total = (uint32_t)D * bits;
+  if (bits > 1) index ^= dilate<D>(low_ones64(bits), bits) >> 1;  // bit 0 of every level, shifted
+  for (uint32_t s = 1; s < total; s *= 2) index ^= index >> s;
+  return index & low_ones64(total);
+}
+
 template <int D>
 __host__ __device__ inline uint64_t hilbert_index_t(uint32_t bits, const int64_t* coord) {
   if (D <= 1) return (uint64_t)coord[0];
-  constexpr uint32_t dims = (uint32_t)D;
-  const uint32_t total = dims * bits;
-  uint64_t packed = 0;
-  for (int d = D - 1; d >= 0; --d) {
-    packed = (packed << bits) | (uint64_t)coord[d];
-  }
-  // transpose: level b holds bit b of every coordinate (coordinate d at bit d)
-  uint64_t t = 0;
-  const uint64_t field = low_ones64(bits);
-  for (uint32_t d = 0; d < dims; ++d) t |= dilate<D>((packed >> (d * bits)) & field, bits) << d;
+  uint64_t t = hilbert_transpose<D>(bits, coord);
   uint64_t index;
   if (bits > 1) {
-    constexpr uint64_t nd_ones = (1ull << dims) - 1ull;
-    constexpr uint64_t nd1_ones = nd_ones >> 1;
-    const uint64_t level_low = dilate<D>(field, bits);  // bit 0 of every level
-    t ^= t >> dims;
+    t ^= t >> D;
     index = 0;
     uint32_t rot = 0;
     uint64_t flip = 0;
-    for (int lvl = (int)bits - 1; lvl >= 0; --lvl) {
-      uint64_t g = ((t >> (lvl * dims)) & nd_ones) ^ flip;
-      if (rot) g = ((g >> rot) | (g << (dims - rot))) & nd_ones;
-      index = (index << dims) | g;
-      flip = 1ull << rot;
-      // the rotation advances past the lowest set bit of g below the top one
-      const uint64_t low = g & (0ull - g) & nd1_ones;
-      if (low) rot += 64u - clz64(low);
-      if (++rot >= dims) rot -= dims;
-    }
-    index ^= level_low >> 1;
+    for (int lvl = (int)bits - 1; lvl >= 0; --lvl)
+      index = (index << D) | hilbert_step<D>((t >> (lvl * D)) & ((1ull << D) - 1ull), rot, flip);
   } else {
     index = t;
   }
-  for (uint32_t s = 1; s < total; s *= 2) index ^= index >> s;
-  return index & low_ones64(total);
+  return hilbert_finish<D>(index, bits);
+}
+
+// Table-driven levels for D = 2 and 3: kHilbertLevels<D> levels per lookup.
+// A rotation state (rot, flip) is encoded as rot * (D + 1) + f, f = 0 for
+// flip == 0 and 1 + log2(flip) otherwise.  Entry [state << (L*D) | input]
+// holds the L*D index bits of the L levels in its low byte and the state
+// after them in bits 8..15; it is filled from hilbert_step, so a lookup is
+// exactly L steps.
+template <int D> struct HilbertTab;
+template <> struct HilbertTab<2> { static constexpr uint32_t L = 4, kStates = 6; };
+template <> struct HilbertTab<3> { static constexpr uint32_t L = 2, kStates = 12; };
+
+template <int D>
+__host__ __device__ __forceinline__ uint16_t hilbert_tab_entry(uint32_t e) {
+  constexpr uint32_t L = HilbertTab<D>::L, IB = L * D;
+  const uint32_t state = e >> IB, in = e & ((1u << IB) - 1u);
+  uint32_t rot = state / (D + 1), f = state % (D + 1);
+  uint64_t flip = f ? (1ull << (f - 1)) : 0ull;
+  uint32_t out = 0;
+  for (uint32_t j = 0; j < L; ++j) {
+    const uint64_t gin = (in >> ((L - 1 - j) * D)) & ((1u << D) - 1u);
+    out = (out << D) | (uint32_t)hilbert_step<D>(gin, rot, flip);
+  }
+  const uint32_t nf = flip ? (uint32_t)(63u - clz64(flip)) + 1u : 0u;
+  return (uint16_t)(out | ((rot * (D + 1) + nf) << 8));
+}
+
+// hilbert_index_t through a filled table (HilbertTab<D>::kStates << (L*D)
+// entries of hilbert_tab_entry), then plain steps for the bits % L lowest
+// levels.
+template <int D>
+__host__ __device__ __forceinline__ uint64_t hilbert_index_tab(uint32_t bits, const int64_t* coord,
+                                                             const uint16_t* tab) {
+  constexpr uint32_t L = HilbertTab<D>::L, IB = L * D;
+  uint64_t t = hilbert_transpose<D>(bits, coord);
+  if (bits <= 1) return hilbert_finish<D>(t, bits);
+  t ^= t >> D;
+  uint64_t index = 0;
+  uint32_t state = 0;
+  int lvl = (int)bits - 1;
+  for (; lvl + 1 >= (int)L; lvl -= (int)L) {
+    const uint32_t in = (uint32_t)(t >> ((lvl + 1 - (int)L) * D)) & ((1u << IB) - 1u);
+    const uint32_t e = tab[(state << IB) | in];
+    index = (index << IB) | (e & 0xffu);
+    state = e >> 8;
+  }
+  uint32_t rot = state / (D + 1), f = state % (D + 1);
+  uint64_t flip = f ? (1ull << (f - 1)) : 0ull;
+  for (; lvl >= 0; --lvl)
+    index = (index << D) | hilbert_step<D>((t >> (lvl * D)) & ((1ull << D) - 1ull), rot, flip);
+  return hilbert_finish<D>(index, bits);
 }
 
 __host__ __device__ inline uint64_t hilbert_index(uint32_t dims, uint32_t bits, const int64_t* coord) {
