@@ -553,9 +553,9 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
   // The first kPrefetch ids of window g + gridDim.x are copied into s.pf
   // while window g is enumerated: their 16-byte-aligned middle [a0, a1) by
   // one bulk copy (thread 0, completing on s.bar, one barrier phase per
-  // window even when it is empty); the up to 3 + 3 ids around it are read
-  // from global memory when the bits are set.  Every thread waits on s.bar
-  // itself, so the prefetched ids need no CTA barrier.
+  // window even when it is empty); the up to 3 + 3 ids around it are loaded
+  // into registers by threads 0..5 and written to s.pf by store_edge.  Every
+  // thread waits on s.bar itself, so the bulk part needs no CTA barrier.
   auto prefetch_range = [&](unsigned long long o, uint32_t sz, unsigned long long* a0,
                             unsigned long long* a1) {
     const uint32_t n = sz < kPrefetch ? sz : kPrefetch;
@@ -563,13 +563,35 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     *a1 = (o + n) & ~3ull;
     if (*a1 < *a0) *a1 = *a0;
   };
+  // The up to 3 + 3 ids around the bulk part: threads 0..5 load one each
+  // into a register when the prefetch is issued and store it into s.pf only
+  // before the window's last barrier, so the load's latency is hidden behind
+  // the enumeration.
+  int32_t edge_v = 0;
+  int32_t edge_at = -1;  // s.pf slot of this thread's edge id, -1: none
   auto prefetch = [&](unsigned long long o, uint32_t sz) {
     unsigned long long a0, a1;
     prefetch_range(o, sz, &a0, &a1);
+    const unsigned long long al = o & ~3ull;
     if (tid == 0) {
       mbar_arrive_expect_tx(&s.bar, (uint32_t)(a1 - a0) * 4u);
-      if (a1 > a0) bulk_copy_g2s(&s.pf[a0 - (o & ~3ull)], src + a0, (uint32_t)(a1 - a0) * 4u, &s.bar);
+      if (a1 > a0) bulk_copy_g2s(&s.pf[a0 - al], src + a0, (uint32_t)(a1 - a0) * 4u, &s.bar);
     }
+    const unsigned long long end = o + (sz < kPrefetch ? sz : kPrefetch);
+    const unsigned long long h1 = a0 < end ? a0 : end;          // head [o, h1)
+    const unsigned long long t0 = a1 > h1 ? a1 : h1;            // tail [t0, end)
+    unsigned long long e = ~0ull;
+    if (tid < 3 && o + tid < h1) e = o + tid;
+    else if (tid >= 3 && tid < 6 && t0 + (tid - 3) < end) e = t0 + (tid - 3);
+    edge_at = -1;
+    if (e != ~0ull) {
+      edge_v = __ldcs(src + e);
+      edge_at = (int32_t)(e - al);
+    }
+  };
+  auto store_edge = [&]() {
+    if (edge_at >= 0) s.pf[edge_at] = edge_v;
+    edge_at = -1;
   };
   uint32_t phase = 0;
   uint32_t size = 0;
@@ -579,6 +601,8 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     off = wbase[blockIdx.x];
     prefetch(off, size);
   }
+  store_edge();
+  __syncthreads();
   for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
     const uint32_t gn = g + gridDim.x;
     uint32_t nsize = 0;
@@ -601,11 +625,8 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     //    rest in rounds whose loads are all issued before the first atomic
     if (size >= 2 && ok) {
       const uint32_t npf = size < kPrefetch ? size : kPrefetch;
-      unsigned long long a0, a1;
-      prefetch_range(off, size, &a0, &a1);
-      const uint32_t i0 = (uint32_t)(a0 - off), i1 = (uint32_t)(a1 - off);  // [i0, i1) in s.pf
       for (uint32_t i = tid; i < npf; i += kRankThreads) {
-        const uint32_t x = (uint32_t)((i >= i0 && i < i1) ? s.pf[i + sh] : __ldcs(in + i)) - lo;
+        const uint32_t x = (uint32_t)s.pf[i + sh] - lo;
         atomicOr(&s.bm[bm_at<BITS>(x >> 5)], 1u << (x & 31));
       }
       for (uint32_t i0 = kPrefetch; i0 < size; i0 += kBatch * kRankThreads) {
@@ -622,7 +643,7 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
             atomicOr(&s.bm[bm_at<BITS>(a[k] >> 5)], 1u << (a[k] & 31));
       }
     } else if (size == 1 && tid == 0) {
-      dst[0] = in[0];
+      dst[0] = s.pf[sh];
     }
     if (__syncthreads_or(!ok)) {  // bitmap complete; s.pf free
       // a bulk copy did not complete in time: flag it and stop (the results
@@ -633,6 +654,8 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     }
     if (gn < total) prefetch(noff, nsize);
     if (size < 2) {
+      store_edge();
+      __syncthreads();  // the next window's edge ids are in place
       size = nsize;
       off = noff;
       continue;  // uniform over the CTA
@@ -684,6 +707,7 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
       dst[pos + k] = (int32_t)(base + __ffs(cur));
       cur &= cur - 1;
     }
+    store_edge();              // the next window's edge ids, before the last barrier
     fence_proxy_async_smem();  // the stage's writes before the bulk store reads them
     __syncthreads();
     // 3. staged ranks out: the 16-byte-aligned middle by one bulk store, the
