@@ -397,8 +397,7 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t nw = (G <= kPerWarpMaxG) ? kTileWarps : 1u;  // counter sets
   unsigned long long* gstart = reinterpret_cast<unsigned long long*>(smem_raw);  // [G]
-  uint32_t* lbase = reinterpret_cast<uint32_t*>(gstart + G);                   // [G]
-  uint32_t* cnt = lbase + G;                                                    // [nw][G]
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(gstart + G);                     // [nw][G]
   uint32_t* stage = cnt + nw * G;                                               // [kTile]
   __shared__ uint32_t wt[kTileWarps];
   const uint32_t lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
@@ -441,14 +440,15 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
     for (uint32_t k = 0; k < per; ++k) {
       const uint32_t w = w0 + k;
       if (w < G) {
-        lbase[w] = run;
         uint32_t tot = 0;
         for (uint32_t q = 0; q < nw; ++q) {
           const uint32_t c = cnt[q * G + w];
           cnt[q * G + w] = run + tot;  // first slot of this counter set in the tile
           tot += c;
         }
-        if (tot) gstart[w] = atomicAdd(&wcur[(size_t)j * G + w], (unsigned long long)tot);
+        // output position of the tile's id at stage slot i of window w:
+        // gstart[w] + i (the window's start minus its local base)
+        if (tot) gstart[w] = atomicAdd(&wcur[(size_t)j * G + w], (unsigned long long)tot) - run;
         run += tot;
       }
     }
@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restr
     for (uint32_t i = threadIdx.x; i < n; i += kTileThreads) {
       const uint32_t id = stage[i];
       const uint32_t w = id >> wbits;
-      dst[gstart[w] + (i - lbase[w])] = (int32_t)id;
+      dst[gstart[w] + i] = (int32_t)id;
     }
     __syncthreads();
   }
@@ -858,7 +858,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   const uint32_t G = 1u << (idbits - wbits);
   const uint32_t sms = (uint32_t)num_sms();
   const uint32_t nsets = (G <= kPerWarpMaxG) ? kTileWarps : 1u;
-  const size_t scatter_bytes = (size_t)G * (8 + 4 + 4 * nsets) + kTile * 4;
+  const size_t scatter_bytes = (size_t)G * (8 + 4 * nsets) + kTile * 4;
 
   // tables per (job, window): counts (u32), bases and cursors (u64); tiles
   // and tile offsets per job
@@ -954,7 +954,7 @@ qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void*
   const size_t scatter_max = (size_t)(1u << (31 - kWinBits)) * 16 + kTile * 4;
   QCP_TRY(set_sort_attrs(ix, scatter_max));
   const uint32_t nsets = (G <= kPerWarpMaxG) ? kTileWarps : 1u;
-  const size_t scatter_bytes = (size_t)G * (8 + 4 + 4 * nsets) + kTile * 4;
+  const size_t scatter_bytes = (size_t)G * (8 + 4 * nsets) + kTile * 4;
   uint32_t* ctr = ws->ctr;
   Job* small = reinterpret_cast<Job*>(ws->jobs[0]);
   Job* big = reinterpret_cast<Job*>(ws->jobs[1]);
