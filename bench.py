@@ -223,7 +223,10 @@ def load_workload(W, name, queries, world):
 
 
 def tune_sample(W, name, w, n=2000):
-    """A query sample of the workload's distribution, with its own seed."""
+    """A query sample of the workload's distribution, with its own seed: at
+    least n queries and a fifth of the workload's batch, so that a trial's
+    time is the batch's work rather than the per-call overhead."""
+    n = max(n, len(w.boxes) // 5) if w.boxes is not None else n
     seed = W.QUERY_SEED + 77
     if name == "uniform1m":
         return W.fixed_cubes(n, 3, 0.0464, seed=seed)
@@ -265,7 +268,7 @@ def run_ours(args, rank, world, local):
     tune = None
     if args.algo == "batched" and not args.no_tune:
         sample = tune_sample(W, args.workload, w)
-        tune = qcp.autotune(w.objs, sample, is_rect=w.is_rect, dims=w.dims, repeats=2)
+        tune = qcp.autotune(w.objs, sample, is_rect=w.is_rect, dims=w.dims, repeats=3)
         knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch", "lanes_per_item",
                                       "hit_cache")}
     args.fanout = knobs["fanout"]
@@ -609,7 +612,7 @@ def run_ours(args, rank, world, local):
             "leaf_prefetch": knobs["leaf_prefetch"] or 2,
             "lanes_per_item": knobs["lanes_per_item"] or 32,
             "hit_cache": "off" if knobs["hit_cache"] == 1 else "on",
-            "tuned": None if tune is None else {"sample_queries": 2000, "best_ms": round(tune["best_ms"], 3),
+            "tuned": None if tune is None else {"sample_queries": int(len(sample)), "best_ms": round(tune["best_ms"], 3),
                                                 "trial_fields": ["fanout", "blocks_per_sm", "win_bits",
                                                                  "leaf_prefetch", "lanes_per_item", "hit_cache", "ms"],
                                                 "trials": [[t["fanout"], t["blocks_per_sm"], t["win_bits"],
@@ -713,7 +716,7 @@ def measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind):
              "hit_cache": 0}
     tune = None
     if not args.no_tune:
-        tune = qcp.autotune(w.objs, tune_sample(W, name, w), is_rect=w.is_rect, dims=w.dims, repeats=2)
+        tune = qcp.autotune(w.objs, tune_sample(W, name, w), is_rect=w.is_rect, dims=w.dims, repeats=3)
         knobs = {k: tune[k] for k in ("fanout", "blocks_per_sm", "win_bits", "leaf_prefetch", "lanes_per_item",
                                       "hit_cache")}
     build = dict(fanout=knobs["fanout"], dims=w.dims, n=w.n, is_rect=w.is_rect, key_bits=w.key_bits, stream=sp)
