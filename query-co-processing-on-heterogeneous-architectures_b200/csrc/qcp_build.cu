@@ -157,12 +157,18 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(
   uint64_t k[RS_ITEMS];
   uint32_t v[RS_ITEMS];
   uint32_t rank[RS_ITEMS];
+  // every load of the tile in flight before the first ranking step
 #pragma unroll
   for (int r = 0; r < RS_ITEMS; ++r) {
     const uint32_t li = w * RS_PER_WARP + r * 32 + lane;
     const bool valid = li < tile_n;
-    k[r] = valid ? keys_in[base + li] : 0ull;
-    v[r] = valid ? vals_in[base + li] : 0u;
+    k[r] = valid ? __ldcs(keys_in + base + li) : 0ull;
+    v[r] = valid ? __ldcs(vals_in + base + li) : 0u;
+  }
+#pragma unroll
+  for (int r = 0; r < RS_ITEMS; ++r) {
+    const uint32_t li = w * RS_PER_WARP + r * 32 + lane;
+    const bool valid = li < tile_n;
     rank[r] = 0;
     const uint32_t active = __ballot_sync(0xffffffffu, valid);
     if (valid) {
