@@ -685,28 +685,14 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     uint32_t cur = 0, base = 0;
     const uint32_t nst = pos < kStage ? min(cnt, kStage - pos) : 0u;
     int32_t* st = s.stage + sh + pos;
-    // the next nonzero word of this thread's range, taken (and cleared) when
-    // the current one is used up
-    auto fetch = [&]() {
-      const uint32_t wi = __ffs(nz) - 1;
-      nz &= nz - 1;
-      cur = s.bm[wi * kRankThreads + tid];
-      s.bm[wi * kRankThreads + tid] = 0u;
-      base = lo + ((tw0 + wi) << 5) - 1;
-    };
-    uint32_t k = 0;
-    for (; k + 2 <= nst; k += 2) {  // two ranks per trip: half the loop overhead
-      if (cur == 0) fetch();
-      const int32_t a = (int32_t)(base + __ffs(cur));
-      cur &= cur - 1;
-      if (cur == 0) fetch();
-      const int32_t b = (int32_t)(base + __ffs(cur));
-      cur &= cur - 1;
-      st[k] = a;
-      st[k + 1] = b;
-    }
-    if (k < nst) {
-      if (cur == 0) fetch();
+    for (uint32_t k = 0; k < nst; ++k) {
+      if (cur == 0) {
+        const uint32_t wi = __ffs(nz) - 1;
+        nz &= nz - 1;
+        cur = s.bm[wi * kRankThreads + tid];
+        s.bm[wi * kRankThreads + tid] = 0u;
+        base = lo + ((tw0 + wi) << 5) - 1;
+      }
       st[k] = (int32_t)(base + __ffs(cur));
       cur &= cur - 1;
     }
