@@ -115,37 +115,43 @@ def dist_setup(n_gpus):
     return rank, world, local
 
 
-def algorithmic_bytes(st: dict, dims: int, fanout: int, is_rect: bool = False) -> dict:
+def algorithmic_bytes(st: dict, dims: int, fanout: int, is_rect: bool = False, hit_cache: bool = True) -> dict:
     """Bytes each kernel must move at minimum for the work it did, per launch
     (one launch of each per step):
     k_leafscan<count>  leaf-MBR reads of every (query, leaf-parent) item +
-                       coordinates of partially covered leaves
-    k_leafscan<write>  the same reads again + 4 B id read and 4 B id write per hit
+                       coordinates of partially covered leaves (+ with the hit
+                       cache, its records written: 12 B per item and 32-leaf
+                       group, 16 B per partial leaf and 128-object chunk)
+    k_leafscan<write>  with the hit cache: those records read back + 4 B id
+                       read and 4 B id write per hit; without it the count
+                       pass's MBR and coordinate reads again + 8 B per hit
     k_sort_small       4 B read + 4 B write per id of the slices <= 8192 ids
     k_win_sort         4 B read + 4 B write per id of the larger slices
     """
     mbr = st["leaf_items"] * fanout * 2 * dims * 4
     coords = st["leaves_partial"] * fanout * (2 if is_rect else 1) * dims * 4
+    cache = (st["leaf_items"] * ((fanout + 31) // 32) * 12
+             + st["leaves_partial"] * ((fanout + 127) // 128) * 16) if hit_cache else 0
     hits = st["hits"]
     win = st["sort_window_ids"]
-    return {"count": mbr + coords, "write": mbr + coords + 8 * hits,
+    return {"count": mbr + coords + cache, "write": (cache if hit_cache else mbr + coords) + 8 * hits,
             "sort_small": 8 * (hits - win), "sort_windows": 8 * win}
 
 
 # DRAM bytes (read + write) per id of k_win_sort measured by ncu on the
 # 16M-point Gaussian workload at 2,000 queries, applied to the ids of the
 # timed launch: traffic grows with the ids processed.
-K_WIN_SORT_DRAM_BYTES_PER_ID = (849777408 + 803374592) / 211501325  # 7.82 B per id
+K_WIN_SORT_DRAM_BYTES_PER_ID = (855284480 + 801693952) / 211501325  # 7.83 B per id
 
 KERNEL_NAMES = {"count": "k_leafscan<count>", "write": "k_leafscan<write>",
                 "sort_small": "k_sort_small", "sort_windows": "k_win_sort"}
 
 
-def roofline_of(stats, phase, steps, dims, fanout, is_rect, hbm, peak_kind):
+def roofline_of(stats, phase, steps, dims, fanout, is_rect, hbm, peak_kind, hit_cache=True):
     """HBM roofline of the step's dominant kernel: algorithmic bytes of one
     launch / that launch's CUDA-event time (the library's phase events on
     the launching stream), against the measured copy bandwidth."""
-    ab = algorithmic_bytes(stats, dims, fanout, is_rect)
+    ab = algorithmic_bytes(stats, dims, fanout, is_rect, hit_cache)
     dominant = max(KERNEL_NAMES, key=lambda k: phase[k])
     per_launch_ms = phase[dominant] / steps
     achieved = ab[dominant] / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
@@ -337,7 +343,8 @@ def run_ours(args, rank, world, local):
     # every candidate is ONE kernel launched once per step, timed by the
     # library's CUDA events on the launching stream
     hbm, peak_kind = peaks()
-    roof = roofline_of(stats, phase, args.steps, w.dims, args.fanout, w.is_rect, hbm, peak_kind)
+    roof = roofline_of(stats, phase, args.steps, w.dims, args.fanout, w.is_rect, hbm, peak_kind,
+                       hit_cache=knobs["hit_cache"] != 1)
 
     # ---- parity of the timed batch (after the timed region) -----------------
     res = ix.search(d_boxes, q=Q, algo=args.algo, result_mem=qcp.MEM_DEVICE, stream=sp,
@@ -762,7 +769,8 @@ def measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind):
         ms, phase, stats = timed("batched", args.steps, timing=True)
     clk = clocks.summary()
     value = Q * args.steps / (ms / 1e3)
-    roof = roofline_of(stats, phase, args.steps, w.dims, knobs["fanout"], w.is_rect, hbm, peak_kind)
+    roof = roofline_of(stats, phase, args.steps, w.dims, knobs["fanout"], w.is_rect, hbm, peak_kind,
+                       hit_cache=knobs["hit_cache"] != 1)
     plain = None
     if args.plain_steps > 0:
         pms, _, _ = timed("plain", args.plain_steps)
