@@ -498,6 +498,13 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // Generic-proxy writes to shared memory before async-proxy reads of them.
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
+// Bit position of the highest set bit of x (x != 0).
+__device__ __forceinline__ uint32_t bfind32(uint32_t x) {
+  uint32_t b;
+  asm("bfind.u32 %0, %1;" : "=r"(b) : "r"(x));
+  return b;
+}
+
 // Position of bitmap word w in shared memory (see k_win_sort).
 template <uint32_t BITS>
 __device__ __forceinline__ uint32_t bm_at(uint32_t w) {
@@ -510,17 +517,21 @@ __device__ __forceinline__ uint32_t bm_at(uint32_t w) {
 //      ids were brought into shared memory by a bulk copy (the TMA unit)
 //      while the previous window ran;
 //   2. every thread owns kLaneWords bitmap words: it counts their set bits,
-//      takes its exclusive prefix over the CTA (warp scan + warp sums), then
-//      walks its nonzero words in order and emits the id of every set bit at
-//      the next rank, clearing each word it read; ranks below kStage go to a
-//      shared-memory stage, larger ones straight to the output;
+//      takes its exclusive prefix over the CTA (warp scan + warp sums), i.e.
+//      its ranks [pos, pos + cnt), then walks its nonzero words from the
+//      highest down and emits the id of every set bit from its highest rank
+//      down (bfind finds the highest set bit in one instruction), clearing
+//      each word it read; ranks below kStage go to a shared-memory stage,
+//      larger ones straight to the output;
 //   3. the stage leaves by one bulk store (its 16-byte-aligned middle) and a
 //      few plain stores (the ends).
-// Three CTA barriers per window: bitmap complete, warp sums ready, stage
-// complete (which also orders the bitmap's clearing before the next
-// window's bits).  The ids of a window are distinct, so the set bits are the
-// window's ids and their enumeration in bit order is the window in
-// ascending order.
+// Warp 0 alone issues the next window's prefetch and the copy-out (their
+// 64-bit offset arithmetic is per CTA, not per thread).  Three CTA barriers
+// per window: bitmap complete, warp sums ready, stage complete (which also
+// orders the bitmap's clearing before the next window's bits).  The ids of a
+// window are distinct, so the set bits are the window's ids and their
+// enumeration in bit order is the window in ascending order.  G is a power
+// of two.
 template <uint32_t BITS>
 __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     k_win_sort(const uint32_t* __restrict__ njobs_p, uint32_t G, uint32_t wbits, const uint32_t* __restrict__ whist,
@@ -599,7 +610,7 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
   if (blockIdx.x < total) {
     size = whist[blockIdx.x];
     off = wbase[blockIdx.x];
-    prefetch(off, size);
+    if (wp == 0) prefetch(off, size);
   }
   store_edge();
   __syncthreads();
@@ -613,7 +624,7 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     }
     const int32_t* in = src + off;
     int32_t* dst = out + off;
-    const uint32_t lo = (g % G) << wbits;
+    const uint32_t lo = (g & (G - 1)) << wbits;
     const uint32_t sh = (uint32_t)(off & 3);  // 16-byte alignment offset of this window's ids
     // this window's prefetched ids (every thread waits itself; the bitmap
     // was cleared and the stage written before the previous window's last
@@ -652,7 +663,7 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
       mbar_wait_bounded(&s.bar, phase ^ 1u);
       break;
     }
-    if (gn < total) prefetch(noff, nsize);
+    if (gn < total && wp == 0) prefetch(noff, nsize);
     if (size < 2) {
       store_edge();
       __syncthreads();  // the next window's edge ids are in place
@@ -678,42 +689,43 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     const uint32_t ws = lane < kRankWarps ? s.wsum[lane] : 0u;
     uint32_t pos = __reduce_add_sync(0xffffffffu, lane < wp ? ws : 0u) + ex;
     // one iteration per set bit (a flat loop: a warp runs as many iterations
-    // as its lane with the most bits); the next nonzero word is fetched, and
-    // cleared, when the current one is used up.  Ranks below kStage go to the
-    // stage and the rest straight to the output, in two loops so that no
-    // iteration tests the rank.
+    // as its lane with the most bits), from rank pos + cnt - 1 down to pos;
+    // the next lower nonzero word is fetched, and cleared, when the current
+    // one is used up.  Ranks from kStage up go straight to the output, the
+    // rest to the stage, in two loops so that no iteration tests the rank.
     uint32_t cur = 0, base = 0;
-    const uint32_t nst = pos < kStage ? min(cnt, kStage - pos) : 0u;
-    int32_t* st = s.stage + sh + pos;
-    for (uint32_t k = 0; k < nst; ++k) {
+    const uint32_t base0 = lo + (tw0 << 5);  // id of bit 0 of this thread's first word
+    uint32_t r = pos + cnt;
+    const uint32_t split = max(pos, min(r, kStage));  // ranks >= split go straight out
+    auto next_bit = [&]() -> uint32_t {
       if (cur == 0) {
-        const uint32_t wi = __ffs(nz) - 1;
-        nz &= nz - 1;
+        const uint32_t wi = bfind32(nz);
+        nz ^= 1u << wi;
         cur = s.bm[wi * kRankThreads + tid];
         s.bm[wi * kRankThreads + tid] = 0u;
-        base = lo + ((tw0 + wi) << 5) - 1;
+        base = base0 + (wi << 5);
       }
-      st[k] = (int32_t)(base + __ffs(cur));
-      cur &= cur - 1;
+      const uint32_t b = bfind32(cur);
+      cur ^= 1u << b;
+      return base + b;
+    };
+    while (r > split) {
+      const uint32_t id = next_bit();
+      dst[--r] = (int32_t)id;
     }
-    for (uint32_t k = nst; k < cnt; ++k) {
-      if (cur == 0) {
-        const uint32_t wi = __ffs(nz) - 1;
-        nz &= nz - 1;
-        cur = s.bm[wi * kRankThreads + tid];
-        s.bm[wi * kRankThreads + tid] = 0u;
-        base = lo + ((tw0 + wi) << 5) - 1;
-      }
-      dst[pos + k] = (int32_t)(base + __ffs(cur));
-      cur &= cur - 1;
+    int32_t* st = s.stage + sh;
+    while (r > pos) {
+      const uint32_t id = next_bit();
+      st[--r] = (int32_t)id;
     }
     store_edge();              // the next window's edge ids, before the last barrier
     fence_proxy_async_smem();  // the stage's writes before the bulk store reads them
     __syncthreads();
-    // 3. staged ranks out: the 16-byte-aligned middle by one bulk store, the
-    //    up to 3 + 3 ids around it by plain stores
+    // 3. staged ranks out (warp 0): the 16-byte-aligned middle by one bulk
+    //    store, the up to 3 + 3 ids around it by plain stores; windows of
+    //    fewer than 8 ids by plain stores
     const uint32_t ns = size < kStage ? size : kStage;
-    {
+    if (wp == 0) {
       const unsigned long long al = off & ~3ull;
       const unsigned long long b0 = (off + 3) & ~3ull, b1 = (off + ns) & ~3ull;
       if (b1 > b0) {
@@ -722,7 +734,7 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
         if (tid < nh) out[off + tid] = s.stage[sh + tid];
         else if (tid >= 4 && tid - 4 < nt) out[b1 + (tid - 4)] = s.stage[b1 - al + (tid - 4)];
       } else {
-        for (uint32_t k = tid; k < ns; k += kRankThreads) dst[k] = s.stage[sh + k];
+        for (uint32_t k = lane; k < ns; k += 32) dst[k] = s.stage[sh + k];
       }
     }
     size = nsize;
