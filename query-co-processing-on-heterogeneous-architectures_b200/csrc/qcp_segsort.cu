@@ -676,9 +676,9 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     if (owner) {
 #pragma unroll
       for (uint32_t k = 0; k < kLaneWords; ++k) {
-        const uint32_t v = s.bm[k * kRankThreads + tid];
-        cnt += __popc(v);
-        nz |= (v ? 1u : 0u) << k;
+        const uint32_t c = __popc(s.bm[k * kRankThreads + tid]);
+        cnt += c;
+        nz += min(c, 1u) << k;  // bit k: word k is nonzero
       }
     }
     uint32_t wtot;
