@@ -51,19 +51,23 @@ constexpr uint32_t kTileThreads = 256;
 constexpr uint32_t kTileWarps = kTileThreads / 32;
 constexpr uint32_t kPerWarpMaxG = 256;  // per-warp window counters up to this G
 // ---- window sort ------------------------------------------------------------
-// One instantiation per window size 2^BITS ids (BITS = 16, 17, 18): the
-// bitmap fills BITS-dependent shared memory, so smaller windows run more
-// CTAs per SM (3, 6, 12) at the same 48 warps; each thread owns 16 words.
+// One instantiation per window size 2^BITS ids (BITS = 16, 17, 18).  Each
+// thread owns kLaneWords bitmap words (32 for 2^17- and 2^18-id windows, 16
+// for 2^16): a window's per-window bookkeeping is paid per warp, so fewer
+// warps per window cost fewer instructions per id, and more bits per thread
+// even out the enumeration's lanes.  Shared memory sets the resident CTAs per
+// SM (kBlocks: 3, 6, 10); the launch takes the occupancy API's count.
 template <uint32_t BITS>
 struct WinCfg {
   static constexpr uint32_t kWords = (1u << BITS) / 32;            // bitmap words
-  static constexpr uint32_t kThreads = kWords / 16;                // 512, 256, 128
+  static constexpr uint32_t kLaneWords = BITS >= 17 ? 32u : 16u;   // bitmap words per thread
+  static constexpr uint32_t kThreads = kWords / kLaneWords;        // 256, 128, 128
   static constexpr uint32_t kWarps = kThreads / 32;
-  static constexpr uint32_t kBlocks = 3u << (18 - BITS);           // resident CTAs per SM
+  static constexpr uint32_t kBlocks = BITS >= 18 ? 3u : (BITS == 17 ? 6u : 10u);  // resident CTAs per SM
+  static constexpr uint32_t kRegBlocks = 49152u / 32u / kThreads;  // launch bound: ~40 registers per thread
   static constexpr uint32_t kStage = BITS >= 18 ? 6144u : (BITS == 17 ? 3072u : 1408u);  // staged output ids
   static constexpr uint32_t kPrefetch = 4096u >> (18 - BITS);      // ids of the next window loaded ahead
 };
-constexpr uint32_t kLaneWords = 16;                    // bitmap words per thread
 constexpr uint32_t kBatch = 8;                         // ids per thread per load round
 constexpr uint32_t kNone = 0xffffffffu;                // empty register slot
 
@@ -508,7 +512,7 @@ __device__ __forceinline__ uint32_t bfind32(uint32_t x) {
 // Position of bitmap word w in shared memory (see k_win_sort).
 template <uint32_t BITS>
 __device__ __forceinline__ uint32_t bm_at(uint32_t w) {
-  return (w % kLaneWords) * WinCfg<BITS>::kThreads + w / kLaneWords;
+  return (w % WinCfg<BITS>::kLaneWords) * WinCfg<BITS>::kThreads + w / WinCfg<BITS>::kLaneWords;
 }
 
 // Persistent CTAs over the (job, window) pairs g = job * G + window.
@@ -533,7 +537,7 @@ __device__ __forceinline__ uint32_t bm_at(uint32_t w) {
 // enumeration in bit order is the window in ascending order.  G is a power
 // of two.
 template <uint32_t BITS>
-__global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
+__global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kRegBlocks)
     k_win_sort(const uint32_t* __restrict__ njobs_p, uint32_t G, uint32_t wbits, const uint32_t* __restrict__ whist,
                const unsigned long long* __restrict__ wbase, const int32_t* __restrict__ src,
                int32_t* __restrict__ out, uint32_t* err) {
@@ -549,6 +553,7 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
   const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   uint4* bm4 = reinterpret_cast<uint4*>(s.bm);
   const uint32_t nwords = (1u << wbits) >> 5;   // 12 <= wbits <= BITS
+  constexpr uint32_t kLaneWords = C::kLaneWords;
   const uint32_t tw0 = tid * kLaneWords;        // this thread's words [tw0, tw0 + kLaneWords)
   const bool owner = tw0 < nwords;
   // Word w of the bitmap (thread w / kLaneWords's word w % kLaneWords) is
@@ -773,7 +778,23 @@ static void launch_win_sort_t(uint64_t max_pairs, uint32_t sms, const uint32_t* 
                               const uint32_t* whist, const unsigned long long* wbase, const int32_t* src,
                               int32_t* out, uint32_t* err, cudaStream_t s) {
   using C = WinCfg<BITS>;
-  const uint64_t cap = (uint64_t)sms * C::kBlocks;
+  // resident CTAs per SM from the occupancy API (its shared memory decides),
+  // once per device and thread
+  static thread_local int occ_dev = -1;
+  static thread_local uint32_t occ = C::kBlocks;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && dev != occ_dev) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_win_sort<BITS>, C::kThreads, sizeof(RankSmem<BITS>)) ==
+            cudaSuccess &&
+        b > 0) {
+      occ = (uint32_t)b;
+      occ_dev = dev;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  const uint64_t cap = (uint64_t)sms * occ;
   const uint32_t grid = (uint32_t)(max_pairs < cap ? max_pairs : cap);
   if (grid)
     k_win_sort<BITS><<<grid, C::kThreads, sizeof(RankSmem<BITS>), s>>>(njobs, G, wbits, whist, wbase, src, out, err);
