@@ -126,7 +126,9 @@ def algorithmic_bytes(st: dict, dims: int, fanout: int, is_rect: bool = False, h
                        read and 4 B id write per hit; without it the count
                        pass's MBR and coordinate reads again + 8 B per hit
     k_sort_small       4 B read + 4 B write per id of the slices <= 8192 ids
-    k_win_sort         4 B read + 4 B write per id of the larger slices
+    k_win_sort         4 B read + 4 B write per id of the windows of more than
+                       512 ids (the larger slices' windows)
+    k_win_sort_warp    the same for their windows of at most 512 ids
     """
     mbr = st["leaf_items"] * fanout * 2 * dims * 4
     coords = st["leaves_partial"] * fanout * (2 if is_rect else 1) * dims * 4
@@ -134,8 +136,9 @@ def algorithmic_bytes(st: dict, dims: int, fanout: int, is_rect: bool = False, h
              + st["leaves_partial"] * ((fanout + 127) // 128) * 16) if hit_cache else 0
     hits = st["hits"]
     win = st["sort_window_ids"]
+    winb = st.get("sort_window_bitmap_ids", win)
     return {"count": mbr + coords + cache, "write": (cache if hit_cache else mbr + coords) + 8 * hits,
-            "sort_small": 8 * (hits - win), "sort_windows": 8 * win}
+            "sort_small": 8 * (hits - win), "sort_windows": 8 * winb, "sort_windows_warp": 8 * (win - winb)}
 
 
 # DRAM bytes (read + write) per id of k_win_sort measured by ncu on the
@@ -144,7 +147,7 @@ def algorithmic_bytes(st: dict, dims: int, fanout: int, is_rect: bool = False, h
 K_WIN_SORT_DRAM_BYTES_PER_ID = (854755584 + 801391104) / 211501325  # 7.83 B per id
 
 KERNEL_NAMES = {"count": "k_leafscan<count>", "write": "k_leafscan<write>",
-                "sort_small": "k_sort_small", "sort_windows": "k_win_sort"}
+                "sort_small": "k_sort_small", "sort_windows": "k_win_sort", "sort_windows_warp": "k_win_sort_warp"}
 
 
 def roofline_of(stats, phase, steps, dims, fanout, is_rect, hbm, peak_kind, hit_cache=True):
@@ -152,12 +155,20 @@ def roofline_of(stats, phase, steps, dims, fanout, is_rect, hbm, peak_kind, hit_
     launch / that launch's CUDA-event time (the library's phase events on
     the launching stream), against the measured copy bandwidth."""
     ab = algorithmic_bytes(stats, dims, fanout, is_rect, hit_cache)
+    # the window phase is two kernels: the bitmap sort (timed between its own
+    # events) and the one-warp sort of the small windows (the rest)
+    phase = dict(phase)
+    if phase.get("sort_windows_bitmap", 0.0) > 0:
+        phase["sort_windows_warp"] = max(0.0, phase["sort_windows"] - phase["sort_windows_bitmap"])
+        phase["sort_windows"] = phase["sort_windows_bitmap"]
+    else:
+        phase["sort_windows_warp"] = 0.0
     dominant = max(KERNEL_NAMES, key=lambda k: phase[k])
     per_launch_ms = phase[dominant] / steps
     achieved = ab[dominant] / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
     traffic = None
     if dominant == "sort_windows" and K_WIN_SORT_DRAM_BYTES_PER_ID:
-        traffic = int(K_WIN_SORT_DRAM_BYTES_PER_ID * stats["sort_window_ids"])
+        traffic = int(K_WIN_SORT_DRAM_BYTES_PER_ID * stats.get("sort_window_bitmap_ids", stats["sort_window_ids"]))
     kernels_gbs = {KERNEL_NAMES[k]: round(ab[k] / (phase[k] / steps / 1e3) / 1e9, 1)
                    for k in KERNEL_NAMES if phase[k] > 0}
     return {"bound": "hbm", "kernel": KERNEL_NAMES[dominant],
@@ -313,7 +324,7 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     qcp.launch_count(reset=True)
     phase = {"expand": 0.0, "count": 0.0, "scan": 0.0, "write": 0.0, "sort": 0.0, "total": 0.0,
-             "sort_small": 0.0, "sort_partition": 0.0, "sort_windows": 0.0}
+             "sort_small": 0.0, "sort_partition": 0.0, "sort_windows": 0.0, "sort_windows_bitmap": 0.0}
     step_ms = []
     stats = None
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -640,7 +651,7 @@ def run_ours(args, rank, world, local):
         "phase_ms_per_step": {k: round(v / args.steps, 4) for k, v in phase.items()},
         "work_per_step": {k: stats[k] for k in ["leaf_items", "leaves_covered", "leaves_partial",
                                                  "objects_covered", "sort_small_jobs", "sort_msd_jobs",
-                                                 "sort_window_ids"]},
+                                                 "sort_window_ids", "sort_window_bitmap_ids"]},
         "roofline": roof,
         "parity": parity,
         "plain": {"value": round(plain, 1) if plain else None, "unit": "queries/s",
@@ -752,7 +763,7 @@ def measure_other(args, qcp, W, name, dev, sp, hbm, peak_kind):
         torch.cuda.synchronize()
         e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         phase = {"expand": 0.0, "count": 0.0, "scan": 0.0, "write": 0.0, "sort": 0.0, "total": 0.0,
-                 "sort_small": 0.0, "sort_partition": 0.0, "sort_windows": 0.0}
+                 "sort_small": 0.0, "sort_partition": 0.0, "sort_windows": 0.0, "sort_windows_bitmap": 0.0}
         e_a.record(stream)
         st = None
         for _ in range(steps):

@@ -172,6 +172,11 @@ typedef struct qcp_query_stats {
   /* parts of ms_sort: small slices, window partition, window sort */
   float ms_sort_small, ms_sort_partition, ms_sort_windows;
   uint64_t sort_window_ids;    /* ids of the slices sorted through windows (with QCP_QUERY_TIMING) */
+  /* the window sort's two kernels: the bitmap sort of the windows of more
+   * than 512 ids (its milliseconds and ids) and the one-warp sort of the
+   * rest (ms_sort_windows minus ms_sort_windows_bitmap) */
+  float ms_sort_windows_bitmap;
+  uint64_t sort_window_bitmap_ids;
 } qcp_query_stats;
 
 qcp_status qcp_query_stats_last(qcp_query_stats* out);

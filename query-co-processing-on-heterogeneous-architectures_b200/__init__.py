@@ -75,7 +75,8 @@ class QueryStats(ctypes.Structure):
                 ("ms_scan", ctypes.c_float), ("ms_write", ctypes.c_float),
                 ("ms_sort", ctypes.c_float), ("ms_total", ctypes.c_float),
                 ("ms_sort_small", ctypes.c_float), ("ms_sort_partition", ctypes.c_float),
-                ("ms_sort_windows", ctypes.c_float), ("sort_window_ids", ctypes.c_uint64)]
+                ("ms_sort_windows", ctypes.c_float), ("sort_window_ids", ctypes.c_uint64),
+                ("ms_sort_windows_bitmap", ctypes.c_float), ("sort_window_bitmap_ids", ctypes.c_uint64)]
 
 
 DELIVER_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int32),

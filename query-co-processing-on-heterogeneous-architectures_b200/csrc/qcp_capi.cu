@@ -638,6 +638,7 @@ static qcp_status run_query(qcp_index* ix, const float* boxes, uint32_t q, const
       t_stats.leaves_partial = ws->h_stats[kStatPartial];
       t_stats.objects_covered = ws->h_stats[kStatObjCovered];
       t_stats.sort_window_ids = ws->h_stats[kStatWindowIds];
+      t_stats.sort_window_bitmap_ids = ws->h_stats[kStatBitmapIds];
       for (int l = 0; l < 16; ++l) t_stats.frontier_items[l] = ws->h_stats[kStatLevel0 + l];
       t_stats.leaf_items = t_stats.frontier_items[1];
       auto ms = [&](int a, int b) {
@@ -660,6 +661,7 @@ static qcp_status run_query(qcp_index* ix, const float* boxes, uint32_t q, const
           if (ws->sort_part_marked) {
             t_stats.ms_sort_partition = ms(kEvSortSmall, kEvSortPart);
             t_stats.ms_sort_windows = ms(kEvSortPart, kEvSort);
+            t_stats.ms_sort_windows_bitmap = ms(kEvSortPart, kEvSortBitmap);
           } else {
             t_stats.ms_sort_windows = ms(kEvSortSmall, kEvSort);
           }

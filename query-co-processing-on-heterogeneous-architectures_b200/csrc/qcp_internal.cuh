@@ -72,7 +72,7 @@ struct DevArray {
 // Phase events of Workspace::ev.
 enum EvSlot : int {
   kEvStart = 0, kEvExpand = 1, kEvCount = 2, kEvScan = 3, kEvWrite = 4, kEvSort = 5,
-  kEvSortSmall = 6, kEvSortPart = 7, kEvCountSlots = 8
+  kEvSortSmall = 6, kEvSortPart = 7, kEvSortBitmap = 8, kEvCountSlots = 9
 };
 
 // Scratch for one query call.  Reused across calls through the index's
@@ -142,6 +142,7 @@ enum StatSlot : uint32_t {
   kStatPartial = 1,     // partially covered leaves (objects tested)
   kStatObjCovered = 2,  // objects in covered leaves
   kStatWindowIds = 3,   // ids of the slices sorted through windows
+  kStatBitmapIds = 4,   // ids of the windows listed for the bitmap sort
   kStatLevel0 = 8,      // frontier items of level l at kStatLevel0 + l
   kStatCount = 24
 };
@@ -164,6 +165,8 @@ enum CtrSlot : uint32_t {
   kCtrWork2 = 8,
   kCtrTimeout = 9,    // nonzero: a bounded device wait ran out (results invalid)
   kCtrMaskWords = 10, // hit-cache words the count pass asked for (may exceed the capacity)
+  kCtrWinBig = 11,    // windows listed for the bitmap sort
+  kCtrWinSmall = 12,  // windows listed for the one-warp sort
   kCtrCount = 16
 };
 

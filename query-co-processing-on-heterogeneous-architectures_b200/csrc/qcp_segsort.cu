@@ -38,6 +38,7 @@ namespace {
 constexpr uint32_t kTinyCap = 1024;                    // ids of a slice sorted by one warp
 constexpr uint32_t kTinyBuckets = 256;                 // buckets of the warp's counting pass
 constexpr uint32_t kTinyWarps = 8;                     // warps per CTA
+constexpr uint32_t kWinWarpMax = 512;                  // windows of at most this many ids: one warp each
 // ---- small slices ----------------------------------------------------------
 constexpr uint32_t kSmallCap = kSmallSliceCap;
 constexpr uint32_t kSmallThreads = 256;
@@ -95,6 +96,69 @@ struct TinySmem {
   uint32_t base[kTinyWarps][kTinyBuckets];
 };
 
+// One warp sorts the size <= kTinyCap distinct ids at src into dst (src may
+// equal dst): buckets by (id - lo) >> bshift (every id's bucket below
+// kTinyBuckets), then the steps above.  The warp's counters are zero on entry
+// and on return.
+__device__ __forceinline__ void warp_bucket_sort(const int32_t* src, int32_t* dst, uint32_t size, uint32_t lo,
+                                                 uint32_t bshift, uint32_t* stage, uint32_t* cnt, uint32_t* base,
+                                                 uint32_t lane) {
+  constexpr uint32_t kPer = kTinyBuckets / 32;  // buckets per lane
+  // 1. the slice into registers (all loads in flight at once), bucket counts
+  constexpr uint32_t kPerLane = kTinyCap / 32;
+  uint32_t v[kPerLane];
+#pragma unroll
+  for (uint32_t k = 0; k < kPerLane; ++k) {
+    const uint32_t i = lane + 32 * k;
+    v[k] = (i < size) ? (uint32_t)__ldg(src + i) : kNone;
+  }
+#pragma unroll
+  for (uint32_t k = 0; k < kPerLane; ++k)
+    if (v[k] != kNone) atomicAdd(&cnt[(v[k] - lo) >> bshift], 1u);
+  __syncwarp();
+  // 2. bucket bases: each lane owns kPer consecutive buckets
+  uint32_t c[kPer];
+  uint32_t t = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kPer; ++k) {
+    c[k] = cnt[lane * kPer + k];
+    t += c[k];
+  }
+  uint32_t tot;
+  uint32_t run = warp_excl_sum(t, &tot);
+#pragma unroll
+  for (uint32_t k = 0; k < kPer; ++k) {
+    base[lane * kPer + k] = run;
+    run += c[k];
+  }
+  __syncwarp();
+  // 3. every id to the next slot of its bucket (order inside a bucket is
+  //    settled below)
+#pragma unroll
+  for (uint32_t k = 0; k < kPerLane; ++k)
+    if (v[k] != kNone) stage[atomicAdd(&base[(v[k] - lo) >> bshift], 1u)] = v[k];
+  __syncwarp();
+  // 4. insertion sort of each bucket [base - count, base); counts cleared
+#pragma unroll
+  for (uint32_t k = 0; k < kPer; ++k) {
+    const uint32_t n = c[k];
+    const uint32_t b0 = base[lane * kPer + k] - n;
+    for (uint32_t i = 1; i < n; ++i) {
+      const uint32_t key = stage[b0 + i];
+      uint32_t jj = i;
+      while (jj > 0 && stage[b0 + jj - 1] > key) {
+        stage[b0 + jj] = stage[b0 + jj - 1];
+        --jj;
+      }
+      stage[b0 + jj] = key;
+    }
+    cnt[lane * kPer + k] = 0;
+  }
+  __syncwarp();
+  for (uint32_t i = lane; i < size; i += 32) __stcs(dst + i, (int32_t)stage[i]);
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(kTinyWarps * 32, 3) k_sort_tiny(const Job* __restrict__ jobs,
                                                                const uint32_t* __restrict__ njobs_p,
                                                                int32_t* out, uint32_t idbits) {
@@ -102,73 +166,73 @@ __global__ void __launch_bounds__(kTinyWarps * 32, 3) k_sort_tiny(const Job* __r
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TinySmem& sm = *reinterpret_cast<TinySmem*>(smem_raw);
   const uint32_t lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-  uint32_t* stage = sm.stage[wp];
-  uint32_t* cnt = sm.cnt[wp];
-  uint32_t* base = sm.base[wp];
-  constexpr uint32_t kPer = kTinyBuckets / 32;  // buckets per lane
+  constexpr uint32_t kPer = kTinyBuckets / 32;
   const uint32_t bshift = idbits > 8 ? idbits - 8 : 0;
 #pragma unroll
-  for (uint32_t k = 0; k < kPer; ++k) cnt[lane * kPer + k] = 0;
+  for (uint32_t k = 0; k < kPer; ++k) sm.cnt[wp][lane * kPer + k] = 0;
   __syncwarp();
   const uint32_t warps = gridDim.x * kTinyWarps;
   for (uint32_t j = blockIdx.x * kTinyWarps + wp; j < njobs; j += warps) {
     const Job jb = jobs[j];
-    const uint32_t size = jb.size;
-    if (size > kTinyCap) continue;  // warp-uniform
-    const int32_t* src = out + jb.off;
-    // 1. the slice into registers (all loads in flight at once), bucket counts
-    constexpr uint32_t kPerLane = kTinyCap / 32;
-    uint32_t v[kPerLane];
+    if (jb.size > kTinyCap) continue;  // warp-uniform
+    warp_bucket_sort(out + jb.off, out + jb.off, jb.size, 0u, bshift, sm.stage[wp], sm.cnt[wp], sm.base[wp], lane);
+  }
+}
+
+// Windows of at most kWinWarpMax ids (listed by k_win_split), one warp
+// each: the window's ids at src + wbase[g] in ascending order to
+// dst + wbase[g], bucketed on their low wbits bits.
+__global__ void __launch_bounds__(kTinyWarps * 32, 3) k_win_sort_warp(const uint32_t* __restrict__ list,
+                                                                   const uint32_t* __restrict__ nlist_p, uint32_t G,
+                                                                   uint32_t wbits, const uint32_t* __restrict__ whist,
+                                                                   const unsigned long long* __restrict__ wbase,
+                                                                   const int32_t* __restrict__ src, int32_t* dst) {
+  const uint32_t nlist = *nlist_p;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TinySmem& sm = *reinterpret_cast<TinySmem*>(smem_raw);
+  const uint32_t lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  constexpr uint32_t kPer = kTinyBuckets / 32;
+  const uint32_t bshift = wbits > 8 ? wbits - 8 : 0;
 #pragma unroll
-    for (uint32_t k = 0; k < kPerLane; ++k) {
-      const uint32_t i = lane + 32 * k;
-      v[k] = (i < size) ? (uint32_t)__ldg(src + i) : kNone;
+  for (uint32_t k = 0; k < kPer; ++k) sm.cnt[wp][lane * kPer + k] = 0;
+  __syncwarp();
+  const uint32_t warps = gridDim.x * kTinyWarps;
+  for (uint32_t i = blockIdx.x * kTinyWarps + wp; i < nlist; i += warps) {
+    const uint32_t g = list[i];
+    const unsigned long long off = wbase[g];
+    const uint32_t lo = (g & (G - 1)) << wbits;
+    warp_bucket_sort(src + off, dst + off, whist[g], lo, bshift, sm.stage[wp], sm.cnt[wp], sm.base[wp], lane);
+  }
+}
+
+// The (job, window) pairs into two lists: windows of 1..kWinWarpMax ids for
+// k_win_sort_warp, larger ones for k_win_sort (one atomic per warp and
+// list).  With big_ids, the ids of the large windows are added to it.
+__global__ void k_win_split(const uint32_t* __restrict__ njobs_p, uint32_t G, const uint32_t* __restrict__ whist,
+                            uint32_t* big, uint32_t* nbig, uint32_t* small, uint32_t* nsmall,
+                            unsigned long long* big_ids) {
+  const uint32_t total = *njobs_p * G;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t g0 = blockIdx.x * blockDim.x; g0 < total; g0 += stride) {  // warp-uniform rounds
+    const uint32_t g = g0 + threadIdx.x;
+    const uint32_t sz = g < total ? whist[g] : 0u;
+    const bool is_small = sz >= 1 && sz <= kWinWarpMax, is_big = sz > kWinWarpMax;
+    const uint32_t ms = __ballot_sync(0xffffffffu, is_small), mb = __ballot_sync(0xffffffffu, is_big);
+    uint32_t bs = 0, bb = 0;
+    if (lane == 0) {
+      if (ms) bs = atomicAdd(nsmall, (uint32_t)__popc(ms));
+      if (mb) bb = atomicAdd(nbig, (uint32_t)__popc(mb));
     }
-#pragma unroll
-    for (uint32_t k = 0; k < kPerLane; ++k)
-      if (v[k] != kNone) atomicAdd(&cnt[v[k] >> bshift], 1u);
-    __syncwarp();
-    // 2. bucket bases: each lane owns kPer consecutive buckets
-    uint32_t c[kPer];
-    uint32_t t = 0;
-#pragma unroll
-    for (uint32_t k = 0; k < kPer; ++k) {
-      c[k] = cnt[lane * kPer + k];
-      t += c[k];
+    bs = __shfl_sync(0xffffffffu, bs, 0);
+    bb = __shfl_sync(0xffffffffu, bb, 0);
+    const uint32_t lt = lane_lt_mask();
+    if (is_small) small[bs + __popc(ms & lt)] = g;
+    if (is_big) big[bb + __popc(mb & lt)] = g;
+    if (big_ids) {
+      const uint32_t ids = __reduce_add_sync(0xffffffffu, is_big ? sz : 0u);
+      if (lane == 0 && ids) atomicAdd(big_ids, (unsigned long long)ids);
     }
-    uint32_t tot;
-    uint32_t run = warp_excl_sum(t, &tot);
-#pragma unroll
-    for (uint32_t k = 0; k < kPer; ++k) {
-      base[lane * kPer + k] = run;
-      run += c[k];
-    }
-    __syncwarp();
-    // 3. every id to the next slot of its bucket (order inside a bucket is
-    //    settled below)
-#pragma unroll
-    for (uint32_t k = 0; k < kPerLane; ++k)
-      if (v[k] != kNone) stage[atomicAdd(&base[v[k] >> bshift], 1u)] = v[k];
-    __syncwarp();
-    // 4. insertion sort of each bucket [base - count, base); counts cleared
-#pragma unroll
-    for (uint32_t k = 0; k < kPer; ++k) {
-      const uint32_t n = c[k];
-      const uint32_t b0 = base[lane * kPer + k] - n;
-      for (uint32_t i = 1; i < n; ++i) {
-        const uint32_t key = stage[b0 + i];
-        uint32_t jj = i;
-        while (jj > 0 && stage[b0 + jj - 1] > key) {
-          stage[b0 + jj] = stage[b0 + jj - 1];
-          --jj;
-        }
-        stage[b0 + jj] = key;
-      }
-      cnt[lane * kPer + k] = 0;
-    }
-    __syncwarp();
-    for (uint32_t i = lane; i < size; i += 32) __stcs(out + jb.off + i, (int32_t)stage[i]);
-    __syncwarp();
   }
 }
 
@@ -515,7 +579,8 @@ __device__ __forceinline__ uint32_t bm_at(uint32_t w) {
   return (w % WinCfg<BITS>::kLaneWords) * WinCfg<BITS>::kThreads + w / WinCfg<BITS>::kLaneWords;
 }
 
-// Persistent CTAs over the (job, window) pairs g = job * G + window.
+// Persistent CTAs over the listed (job, window) pairs g = job * G + window
+// (the windows of more than kWinWarpMax ids).
 //   1. every id of window g (read from src, the scratch buffer) sets its bit
 //      in a bitmap of the window's 2^wbits possible ids; its first kPrefetch
 //      ids were brought into shared memory by a bulk copy (the TMA unit)
@@ -538,16 +603,16 @@ __device__ __forceinline__ uint32_t bm_at(uint32_t w) {
 // of two.
 template <uint32_t BITS>
 __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kRegBlocks)
-    k_win_sort(const uint32_t* __restrict__ njobs_p, uint32_t G, uint32_t wbits, const uint32_t* __restrict__ whist,
-               const unsigned long long* __restrict__ wbase, const int32_t* __restrict__ src,
-               int32_t* __restrict__ out, uint32_t* err) {
+    k_win_sort(const uint32_t* __restrict__ list, const uint32_t* __restrict__ nlist_p, uint32_t G, uint32_t wbits,
+               const uint32_t* __restrict__ whist, const unsigned long long* __restrict__ wbase,
+               const int32_t* __restrict__ src, int32_t* __restrict__ out, uint32_t* err) {
   using C = WinCfg<BITS>;
   constexpr uint32_t kRankThreads = C::kThreads;
   constexpr uint32_t kRankWarps = C::kWarps;
   constexpr uint32_t kBmWords = C::kWords;
   constexpr uint32_t kStage = C::kStage;
   constexpr uint32_t kPrefetch = C::kPrefetch;
-  const uint32_t total = *njobs_p * G;  // (job, window) pairs
+  const uint32_t total = *nlist_p;  // listed (job, window) pairs
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RankSmem<BITS>& s = *reinterpret_cast<RankSmem<BITS>*>(smem_raw);
   const uint32_t tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
@@ -613,17 +678,20 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kRegBloc
   uint32_t size = 0;
   unsigned long long off = 0;
   if (blockIdx.x < total) {
-    size = whist[blockIdx.x];
-    off = wbase[blockIdx.x];
+    const uint32_t g0 = list[blockIdx.x];
+    size = whist[g0];
+    off = wbase[g0];
     if (wp == 0) prefetch(off, size);
   }
   store_edge();
   __syncthreads();
-  for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
-    const uint32_t gn = g + gridDim.x;
+  for (uint32_t li = blockIdx.x; li < total; li += gridDim.x) {
+    const uint32_t g = list[li];
+    const uint32_t ln = li + gridDim.x;  // this CTA's next listed window
     uint32_t nsize = 0;
     unsigned long long noff = 0;
-    if (gn < total) {
+    if (ln < total) {
+      const uint32_t gn = list[ln];
       nsize = whist[gn];
       noff = wbase[gn];
     }
@@ -668,7 +736,7 @@ __global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kRegBloc
       mbar_wait_bounded(&s.bar, phase ^ 1u);
       break;
     }
-    if (gn < total && wp == 0) prefetch(noff, nsize);
+    if (ln < total && wp == 0) prefetch(noff, nsize);
     if (size < 2) {
       store_edge();
       __syncthreads();  // the next window's edge ids are in place
@@ -774,9 +842,9 @@ static uint32_t id_bits(uint64_t n) {
 // The window sort for 2^wbits-id windows (the instantiation whose bitmap
 // holds them), over at most `max_pairs` (job, window) pairs.
 template <uint32_t BITS>
-static void launch_win_sort_t(uint64_t max_pairs, uint32_t sms, const uint32_t* njobs, uint32_t G, uint32_t wbits,
-                              const uint32_t* whist, const unsigned long long* wbase, const int32_t* src,
-                              int32_t* out, uint32_t* err, cudaStream_t s) {
+static void launch_win_sort_t(uint64_t max_pairs, uint32_t sms, const uint32_t* list, const uint32_t* nlist,
+                              uint32_t G, uint32_t wbits, const uint32_t* whist, const unsigned long long* wbase,
+                              const int32_t* src, int32_t* out, uint32_t* err, cudaStream_t s) {
   using C = WinCfg<BITS>;
   // resident CTAs per SM from the occupancy API (its shared memory decides),
   // once per device and thread
@@ -797,15 +865,31 @@ static void launch_win_sort_t(uint64_t max_pairs, uint32_t sms, const uint32_t* 
   const uint64_t cap = (uint64_t)sms * occ;
   const uint32_t grid = (uint32_t)(max_pairs < cap ? max_pairs : cap);
   if (grid)
-    k_win_sort<BITS><<<grid, C::kThreads, sizeof(RankSmem<BITS>), s>>>(njobs, G, wbits, whist, wbase, src, out, err);
+    k_win_sort<BITS><<<grid, C::kThreads, sizeof(RankSmem<BITS>), s>>>(list, nlist, G, wbits, whist, wbase, src, out,
+                                                                       err);
 }
 
-static void launch_win_sort(uint64_t max_pairs, uint32_t sms, const uint32_t* njobs, uint32_t G, uint32_t wbits,
-                            const uint32_t* whist, const unsigned long long* wbase, const int32_t* src, int32_t* out,
-                            uint32_t* err, cudaStream_t s) {
-  if (wbits >= 18) launch_win_sort_t<18>(max_pairs, sms, njobs, G, wbits, whist, wbase, src, out, err, s);
-  else if (wbits == 17) launch_win_sort_t<17>(max_pairs, sms, njobs, G, wbits, whist, wbase, src, out, err, s);
-  else launch_win_sort_t<16>(max_pairs, sms, njobs, G, wbits, whist, wbase, src, out, err, s);
+// The windows of a call: k_win_split lists them (counts in ctr[kCtrWinBig],
+// ctr[kCtrWinSmall], zeroed by the caller), the bitmap sort takes the large
+// ones and one warp each the small ones.  lists holds 2 * max_pairs entries;
+// max_pairs bounds the (job, window) pairs.
+static void launch_win_sort(Workspace* ws, uint64_t max_pairs, uint32_t sms, const uint32_t* njobs, uint32_t G,
+                            uint32_t wbits, const uint32_t* whist, const unsigned long long* wbase, uint32_t* lists,
+                            uint32_t* ctr, const int32_t* src, int32_t* out, uint32_t* err, cudaStream_t s,
+                            bool stats) {
+  uint32_t* big = lists;
+  uint32_t* small = lists + max_pairs;
+  const uint64_t split_blocks = (max_pairs + 255) / 256;
+  k_win_split<<<(uint32_t)(split_blocks < (uint64_t)sms * 8 ? split_blocks : (uint64_t)sms * 8), 256, 0, s>>>(
+      njobs, G, whist, big, ctr + kCtrWinBig, small, ctr + kCtrWinSmall,
+      stats && ws->timing ? ws->d_stats + kStatBitmapIds : nullptr);
+  if (wbits >= 18) launch_win_sort_t<18>(max_pairs, sms, big, ctr + kCtrWinBig, G, wbits, whist, wbase, src, out, err, s);
+  else if (wbits == 17) launch_win_sort_t<17>(max_pairs, sms, big, ctr + kCtrWinBig, G, wbits, whist, wbase, src, out, err, s);
+  else launch_win_sort_t<16>(max_pairs, sms, big, ctr + kCtrWinBig, G, wbits, whist, wbase, src, out, err, s);
+  if (stats) mark(ws, kEvSortBitmap, s);
+  const uint64_t warp_blocks = (max_pairs + kTinyWarps - 1) / kTinyWarps;
+  k_win_sort_warp<<<(uint32_t)(warp_blocks < (uint64_t)sms * 4 ? warp_blocks : (uint64_t)sms * 4), kTinyWarps * 32,
+                    sizeof(TinySmem), s>>>(small, ctr + kCtrWinSmall, G, wbits, whist, wbase, src, out);
 }
 
 static qcp_status set_sort_attrs(const qcp_index* ix, size_t scatter_max) {
@@ -814,6 +898,8 @@ static qcp_status set_sort_attrs(const qcp_index* ix, size_t scatter_max) {
     QCP_CUDA(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(BucketSmem)));
     QCP_CUDA(cudaFuncSetAttribute(k_sort_tiny, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(TinySmem)));
+    QCP_CUDA(cudaFuncSetAttribute(k_win_sort_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(TinySmem)));
     QCP_CUDA(cudaFuncSetAttribute(k_win_sort<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(RankSmem<16>)));
@@ -897,7 +983,8 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   // and tile offsets per job
   const size_t nw = (size_t)nbig * G;
   const size_t hist_bytes = (nw * 4 + 15) & ~(size_t)15;
-  const size_t bytes = hist_bytes + nw * 16 + (size_t)nbig * 8 + 64;
+  const size_t lists_off = (hist_bytes + nw * 16 + (size_t)nbig * 8 + 15) & ~(size_t)15;
+  const size_t bytes = lists_off + nw * 8 + 64;
   void* tables = nullptr;
   QCP_TRY(ix->pool.get(bytes, &tables));
   uint32_t* whist = reinterpret_cast<uint32_t*>(tables);
@@ -905,6 +992,7 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
   unsigned long long* wcur = wbase + nw;
   uint32_t* tiles = reinterpret_cast<uint32_t*>(wcur + nw);
   uint32_t* tile_off = tiles + nbig;
+  uint32_t* lists = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(tables) + lists_off);  // 2 * nw
   qcp_status st = QCP_OK;
   do {
     k_tiles_per_job<<<(nbig + 255) / 256, 256, 0, s>>>(big, ctr + kCtrJobs1, nbig, tiles);
@@ -938,8 +1026,13 @@ qcp_status segmented_sort(qcp_index* ix, Workspace* ws, uint32_t q, cudaStream_t
         big, map, tile_off, ctr + kCtrWork2, ws->out_ids, ws->tmp_ids, G, wbits, wcur);
     mark(ws, kEvSortPart, s);
     ws->sort_part_marked = ws->timing;
-    launch_win_sort(nw, sms, ctr + kCtrJobs1, G, wbits, whist, wbase, ws->tmp_ids, ws->out_ids, ctr + kCtrTimeout, s);
-    note_launch(5);
+    if (cudaMemsetAsync(ctr + kCtrWinBig, 0, 2 * sizeof(uint32_t), s) != cudaSuccess) {
+      st = cuda_status(cudaGetLastError(), "memset");
+      break;
+    }
+    launch_win_sort(ws, nw, sms, ctr + kCtrJobs1, G, wbits, whist, wbase, lists, ctr, ws->tmp_ids, ws->out_ids,
+                    ctr + kCtrTimeout, s, true);
+    note_launch(7);
     st = check_launch("segmented sort windows");
     // the tables go back to the pool below: make sure the kernels are done
     if (st == QCP_OK && cudaStreamSynchronize(s) != cudaSuccess) st = cuda_status(cudaGetLastError(), "sort");
@@ -971,7 +1064,8 @@ size_t sort_tables_bytes(const qcp_index* ix, const Workspace* ws, uint32_t q) {
   uint32_t wbits = 0, G = 0;
   window_shape(ix, ws, &wbits, &G);
   const size_t nw = (size_t)q * G;
-  return ((nw * 4 + 15) & ~(size_t)15) + nw * 16 + (size_t)q * 8 + 64;
+  const size_t lists_off = ((((nw * 4 + 15) & ~(size_t)15) + nw * 16 + (size_t)q * 8) + 15) & ~(size_t)15;
+  return lists_off + nw * 8 + 64;
 }
 
 // segmented_sort without host readbacks: job and tile counts stay on the
@@ -998,6 +1092,8 @@ qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void*
   unsigned long long* wcur = wbase + nw;
   uint32_t* tiles = reinterpret_cast<uint32_t*>(wcur + nw);
   uint32_t* tile_off = tiles + q;
+  const size_t lists_off = (hist_bytes + nw * 16 + (size_t)q * 8 + 15) & ~(size_t)15;
+  uint32_t* lists = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(tables) + lists_off);  // 2 * nw
   QCP_CUDA(cudaMemsetAsync(ctr + kCtrJobs0, 0, sizeof(uint32_t) * 3, s));  // jobs0, jobs1, small
   k_classify<<<(q + 255) / 256, 256, 0, s>>>((const unsigned long long*)ws->offsets, q, small, ctr + kCtrJobs0,
                                              ctr + kCtrSmall, ws->jobs_cap,
@@ -1022,9 +1118,10 @@ qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void*
   k_win_scatter<<<sms * scatter_blocks_per_sm(scatter_bytes), kTileThreads, scatter_bytes, s>>>(
       big, ws->seg_hist, tile_off, ctr + kCtrWork2,
                                                              ws->out_ids, ws->tmp_ids, G, wbits, wcur);
-  launch_win_sort((uint64_t)-1, sms, ctr + kCtrJobs1, G, wbits, whist, wbase, ws->tmp_ids, ws->out_ids,
-                  ctr + kCtrTimeout, s);
-  note_launch(5);
+  QCP_CUDA(cudaMemsetAsync(ctr + kCtrWinBig, 0, 2 * sizeof(uint32_t), s));
+  launch_win_sort(ws, nw, sms, ctr + kCtrJobs1, G, wbits, whist, wbase, lists, ctr, ws->tmp_ids, ws->out_ids,
+                  ctr + kCtrTimeout, s, false);
+  note_launch(7);
   return check_launch("segmented sort (device counts)");
 }
 
