@@ -142,9 +142,10 @@ def algorithmic_bytes(st: dict, dims: int, fanout: int, is_rect: bool = False, h
 
 
 # DRAM bytes (read + write) per id of k_win_sort measured by ncu on the
-# 16M-point Gaussian workload at 2,000 queries, applied to the ids of the
-# timed launch: traffic grows with the ids processed.
-K_WIN_SORT_DRAM_BYTES_PER_ID = (854755584 + 801391104) / 211501325  # 7.83 B per id
+# 16M-point Gaussian workload at 2,000 queries (its windows of more than 512
+# ids), applied to the ids of the timed launch: traffic grows with the ids
+# processed.
+K_WIN_SORT_DRAM_BYTES_PER_ID = (803071488 + 750159104) / 199061408  # 7.80 B per id
 
 KERNEL_NAMES = {"count": "k_leafscan<count>", "write": "k_leafscan<write>",
                 "sort_small": "k_sort_small", "sort_windows": "k_win_sort", "sort_windows_warp": "k_win_sort_warp"}

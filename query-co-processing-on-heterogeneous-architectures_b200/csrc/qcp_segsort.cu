@@ -96,16 +96,18 @@ struct TinySmem {
   uint32_t base[kTinyWarps][kTinyBuckets];
 };
 
-// One warp sorts the size <= kTinyCap distinct ids at src into dst (src may
-// equal dst): buckets by (id - lo) >> bshift (every id's bucket below
-// kTinyBuckets), then the steps above.  The warp's counters are zero on entry
-// and on return.
+// One warp sorts the size <= CAP (<= kTinyCap) distinct ids at src into dst
+// (src may equal dst): buckets by (id - lo) >> bshift (every id's bucket
+// below kTinyBuckets), then the steps above.  The warp's counters are zero
+// on entry and on return.
+template <uint32_t CAP>
 __device__ __forceinline__ void warp_bucket_sort(const int32_t* src, int32_t* dst, uint32_t size, uint32_t lo,
                                                  uint32_t bshift, uint32_t* stage, uint32_t* cnt, uint32_t* base,
                                                  uint32_t lane) {
   constexpr uint32_t kPer = kTinyBuckets / 32;  // buckets per lane
   // 1. the slice into registers (all loads in flight at once), bucket counts
-  constexpr uint32_t kPerLane = kTinyCap / 32;
+  static_assert(CAP % 32 == 0 && CAP <= kTinyCap, "one warp's stage holds kTinyCap ids");
+  constexpr uint32_t kPerLane = CAP / 32;
   uint32_t v[kPerLane];
 #pragma unroll
   for (uint32_t k = 0; k < kPerLane; ++k) {
@@ -175,7 +177,8 @@ __global__ void __launch_bounds__(kTinyWarps * 32, 3) k_sort_tiny(const Job* __r
   for (uint32_t j = blockIdx.x * kTinyWarps + wp; j < njobs; j += warps) {
     const Job jb = jobs[j];
     if (jb.size > kTinyCap) continue;  // warp-uniform
-    warp_bucket_sort(out + jb.off, out + jb.off, jb.size, 0u, bshift, sm.stage[wp], sm.cnt[wp], sm.base[wp], lane);
+    warp_bucket_sort<kTinyCap>(out + jb.off, out + jb.off, jb.size, 0u, bshift, sm.stage[wp], sm.cnt[wp], sm.base[wp],
+                               lane);
   }
 }
 
@@ -201,7 +204,8 @@ __global__ void __launch_bounds__(kTinyWarps * 32, 3) k_win_sort_warp(const uint
     const uint32_t g = list[i];
     const unsigned long long off = wbase[g];
     const uint32_t lo = (g & (G - 1)) << wbits;
-    warp_bucket_sort(src + off, dst + off, whist[g], lo, bshift, sm.stage[wp], sm.cnt[wp], sm.base[wp], lane);
+    warp_bucket_sort<kWinWarpMax>(src + off, dst + off, whist[g], lo, bshift, sm.stage[wp], sm.cnt[wp], sm.base[wp],
+                                  lane);
   }
 }
 
