@@ -394,6 +394,9 @@ struct SortJob {
 
 // Slices of at most this many ids are sorted whole in shared memory.
 constexpr uint32_t kSmallSliceCap = 8192;
+// Ids per tile of the window partition (a tile map holds one entry per tile
+// of the larger slices: at most hits / kSortTile + slices).
+constexpr uint32_t kSortTile = 2048;
 
 // ---------------------------------------------------------------------------
 // Kernel launchers (defined in the .cu files)

@@ -89,7 +89,7 @@ extern "C" qcp_status qcp_plan_create(qcp_index* ix, uint32_t max_queries, uint6
     if ((st = ws_reserve_items(ix, ws, (size_t)max_queries * 64 + (size_t)(max_hits >> 10) + (1u << 16))) != QCP_OK)
       break;
     if ((st = ws_reserve_out(ix, ws, (size_t)max_hits)) != QCP_OK) break;
-    if ((st = ws_reserve_sort(ix, ws, (size_t)max_queries + 256, (size_t)(max_hits / 4096) + max_queries + 1)) !=
+    if ((st = ws_reserve_sort(ix, ws, (size_t)max_queries + 256, (size_t)(max_hits / kSortTile) + max_queries + 1)) !=
         QCP_OK)
       break;
     if (p->sort) {  // the write pass gathers the sort's per-window counts

@@ -47,8 +47,12 @@ constexpr uint32_t kBucketBits = 11;
 constexpr uint32_t kBuckets = 1u << kBucketBits;
 // ---- window partition ------------------------------------------------------
 constexpr uint32_t kWinBits = 18;
-constexpr uint32_t kTile = 4096;
-constexpr uint32_t kTileThreads = 256;
+// 128 threads x 16 ids per tile, 10 CTAs per SM: the partition's per-tile
+// chain (counts, scan, one global atomic per window, barriers) is latency-
+// bound, and more, smaller CTAs keep more chains in flight per SM
+constexpr uint32_t kTile = kSortTile;
+constexpr uint32_t kTileThreads = 128;
+constexpr uint32_t kTileBlocks = 10;  // launch bound of k_win_scatter (registers for 10 CTAs per SM)
 constexpr uint32_t kTileWarps = kTileThreads / 32;
 constexpr uint32_t kPerWarpMaxG = 256;  // per-warp window counters up to this G
 // ---- window sort ------------------------------------------------------------
@@ -459,7 +463,7 @@ __global__ void __launch_bounds__(kTileThreads) k_win_scan(const Job* __restrict
 // G <= kPerWarpMaxG each warp counts into its own counters (the counter's
 // old value is the id's slot among its warp's ids of that window); the
 // order inside a window does not matter, the ranking orders it.
-__global__ void __launch_bounds__(kTileThreads) k_win_scatter(const Job* __restrict__ jobs,
+__global__ void __launch_bounds__(kTileThreads, kTileBlocks) k_win_scatter(const Job* __restrict__ jobs,
                                                               const uint32_t* __restrict__ map,
                                                               const uint32_t* __restrict__ tile_off,
                                                               const uint32_t* __restrict__ ntiles_p, const int32_t* __restrict__ src,
@@ -1074,7 +1078,7 @@ size_t sort_tables_bytes(const qcp_index* ix, const Workspace* ws, uint32_t q) {
 
 // segmented_sort without host readbacks: job and tile counts stay on the
 // device, every launch has a fixed grid and the kernels read the counts.
-// Tables (sort_tables_bytes) and the tile map (at least total/4096 + q
+// Tables (sort_tables_bytes) and the tile map (at least total/kSortTile + q
 // entries, ws->seg_hist) are the caller's.  Stream-capturable.
 qcp_status segmented_sort_device(qcp_index* ix, Workspace* ws, uint32_t q, void* tables, cudaStream_t s) {
   if (q == 0) return QCP_OK;
