@@ -76,8 +76,9 @@ __global__ void k_keys(const float* __restrict__ objs, uint64_t n, uint32_t is_r
 // ---------------------------------------------------------------------------
 // LSD radix sort, 8-bit digits.  Per pass: upsweep (tile histograms), an
 // exclusive scan of the digit-major [256][tiles] table, and a downsweep that
-// ranks each tile stably (warp match + per-warp digit counters), regroups the
-// tile by digit in shared memory and writes each digit run contiguously.
+// ranks each tile stably (the lanes of a warp with the same digit found by 8
+// ballots, one per digit bit, + per-warp digit counters), regroups the tile
+// by digit in shared memory and writes each digit run contiguously.
 // ---------------------------------------------------------------------------
 constexpr int RS_THREADS = 256;
 constexpr int RS_WARPS = RS_THREADS / 32;
@@ -136,7 +137,7 @@ __device__ __forceinline__ uint32_t block_excl_scan256(uint32_t v, uint32_t* war
   return r;
 }
 
-__global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(
+__global__ void __launch_bounds__(RS_THREADS, 5) k_rs_downsweep(
     const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint64_t n, uint32_t shift,
     const uint32_t* __restrict__ offs, uint32_t ntiles) {
@@ -173,7 +174,13 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(
     const uint32_t active = __ballot_sync(0xffffffffu, valid);
     if (valid) {
       const uint32_t d = (uint32_t)(k[r] >> shift) & 255u;
-      const uint32_t peers = __match_any_sync(active, d);
+      uint32_t peers = active;
+#pragma unroll
+      for (int bb = 0; bb < 8; ++bb) {
+        const uint32_t bit = (d >> bb) & 1u;
+        const uint32_t bal = __ballot_sync(active, bit);
+        peers &= bit ? bal : ~bal;
+      }
       const uint32_t prev = wcnt[w][d];
       rank[r] = prev + __popc(peers & lanemask_lt());
       __syncwarp(active);
