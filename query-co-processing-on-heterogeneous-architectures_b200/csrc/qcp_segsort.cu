@@ -21,12 +21,13 @@
 //                              tile regrouped by window in shared memory and
 //                              written as contiguous runs into the scratch
 //                              buffer;
-//                           2. each (slice, window) is ranked through a
-//                              bitmap of its 2^wbits possible ids: every id
-//                              sets its bit, a prefix count over the words
-//                              follows, and every id goes to its rank
-//                              (bits before its word + bits below it in its
-//                              word) -- no comparisons.
+//                           2. each (slice, window) of more than
+//                              kWinWarpMax ids is sorted through a bitmap of
+//                              its 2^wbits possible ids: every id sets its
+//                              bit, every thread counts the set bits of its
+//                              words, and after a CTA prefix enumerates them
+//                              in order -- no comparisons; the smaller
+//                              windows are bucket-sorted by one warp each.
 #include "qcp_internal.cuh"
 #include "qcp_tree.cuh"
 
