@@ -225,6 +225,37 @@ def test_slice_sizes_at_every_sort_boundary(qcp, oracle):
             assert_same_hits(res.offsets, res.ids, want_offs, want_ids, boxes)
 
 
+def test_window_sizes_at_the_one_warp_boundary(qcp, oracle):
+    """Slices of more than 8,192 ids whose 2^17-id windows hold exactly 512
+    and 513 ids (one warp each up to 512, the bitmap above), 1, 2, 511,
+    8,000 and 9,000 ids and none: 2^19 points, so ids [w * 2^17, (w+1) * 2^17)
+    form window w, and two boxes each select chosen ids of every window."""
+    W = 1 << 17
+    n = 4 * W
+    rng = np.random.default_rng(512)
+    per_box = {0: [512, 513, 8000, 1], 1: [0, 2, 9000, 511]}
+    objs = np.zeros((n, 3), np.float32)
+    objs[:, 0] = rng.uniform(0.6, 0.95, n)  # outside both boxes
+    objs[:, 1:] = rng.uniform(0.05, 0.45, (n, 2))
+    free = [rng.permutation(np.arange(w * W, (w + 1) * W)) for w in range(4)]
+    used = [0, 0, 0, 0]
+    for b, sizes in per_box.items():
+        x0 = 0.05 if b == 0 else 0.30
+        for w, k in enumerate(sizes):
+            sel = free[w][used[w]:used[w] + k]
+            used[w] += k
+            objs[sel, 0] = rng.uniform(x0, x0 + 0.15, k)
+    boxes = np.asarray([[0.0, 0.0, 0.0, 0.25, 0.5, 0.5], [0.275, 0.0, 0.0, 0.5, 0.5, 0.5]], np.float32)
+    want_offs, want_ids = oracle.ids(objs, 3, False, boxes)
+    for b, sizes in per_box.items():
+        ids = np.asarray(want_ids[int(want_offs[b]):int(want_offs[b + 1])], np.int64)
+        assert list(np.bincount(ids >> 17, minlength=4)) == sizes
+    with qcp.Index.build(objs) as ix:
+        for algo in ["batched", "plain"]:
+            res = ix.search(boxes, algo=algo, win_bits=17)
+            assert_same_hits(res.offsets, res.ids, want_offs, want_ids, boxes)
+
+
 def test_hit_cache_overflow_then_full(qcp, oracle, workloads):
     """The write pass replays the count pass's leaf masks and hit bits.  The
     first call on a fresh index has room for 2^20 words of hit bits; this
