@@ -70,7 +70,8 @@ struct WinCfg {
   static constexpr uint32_t kThreads = kWords / kLaneWords;        // 256, 128, 128
   static constexpr uint32_t kWarps = kThreads / 32;
   static constexpr uint32_t kBlocks = BITS >= 18 ? 3u : (BITS == 17 ? 6u : 10u);  // resident CTAs per SM
-  static constexpr uint32_t kRegBlocks = 49152u / 32u / kThreads;  // launch bound: ~40 registers per thread
+  // the launch bound: registers for kBlocks CTAs per SM (shared memory allows
+  // no more); tighter caps (~40 registers) measured 5 % slower
   static constexpr uint32_t kStage = BITS >= 18 ? 6144u : (BITS == 17 ? 3072u : 1408u);  // staged output ids
   static constexpr uint32_t kPrefetch = 4096u >> (18 - BITS);      // ids of the next window loaded ahead
 };
@@ -611,7 +612,7 @@ __device__ __forceinline__ uint32_t bm_at(uint32_t w) {
 // enumeration in bit order is the window in ascending order.  G is a power
 // of two.
 template <uint32_t BITS>
-__global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kRegBlocks)
+__global__ void __launch_bounds__(WinCfg<BITS>::kThreads, WinCfg<BITS>::kBlocks)
     k_win_sort(const uint32_t* __restrict__ list, const uint32_t* __restrict__ nlist_p, uint32_t G, uint32_t wbits,
                const uint32_t* __restrict__ whist, const unsigned long long* __restrict__ wbase,
                const int32_t* __restrict__ src, int32_t* __restrict__ out, uint32_t* err) {
